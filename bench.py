@@ -1,0 +1,343 @@
+"""Benchmark of the SE3P k-space solve on B200 (one JSON line on stdout).
+
+Workload (default, the configuration the headline metric is quoted on):
+SE3P FORCE, N = 100,000 charges uniform in the unit box, charges uniform in
+[-1, 1] shifted to zero sum, M = 128^3, P = 16, xi = 20, m = 0.94 sqrt(pi P);
+FP32 spread/interpolation with compensated accumulation, FP64 FFT and
+Green's-function scaling.  A step is one full solve (sort, spread + fold,
+D2Z, scaling, Z2D, unfold + interpolation) of that system.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Timing: W untimed steps, then K steps each timed with CUDA events on the
+solve's stream; a 256 MiB buffer is written between steps so every step
+starts with a cold L2 (the inputs, 3.2 MB, and grids, 50 MB, would fit in it).
+Under torchrun every rank solves its own replica (weak scaling); the time is
+the max over ranks.  `e2e` repeats the measurement through se_solve_host with
+pinned host buffers (H2D of x, q and D2H of the forces inside the timed
+region).  `--impl reference` times SE_fast_gridding's own CPU spectral_ewald()
+(built from its sources) on all host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(N=100_000, M=128, P=16, L=1.0, xi=20.0, mode="force", precision="fp32",
+                charges="uniform", seed=1)
+METRIC = "SE3P particles/s at rel-RMS<=1e-6 vs FP64 oracle; serve solves/s, p50/p99"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_name(w):
+    return (f"SE3P {w['mode'].upper()} N={w['N']} M={w['M']}^3 P={w['P']} xi={w['xi']} "
+            f"L={w['L']}, {w['precision'].upper()} gridding (compensated), FP64 FFT+scaling")
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference(args, procs, threads, steps, warmup, w):
+    cmd = [sys.executable, os.path.join(ROOT, "oracle", "ref_bench.py"),
+           "--N", str(w["N"]), "--M", str(w["M"]), "--P", str(w["P"]), "--L", str(w["L"]),
+           "--xi", str(w["xi"]), "--mode", w["mode"], "--charges", w["charges"],
+           "--seed", str(w["seed"]), "--procs", str(procs), "--threads", str(threads),
+           "--steps", str(steps), "--warmup", str(warmup)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr[-2000:])
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        for ln in self.lines:
+            f = [s.strip() for s in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    w = WORKLOAD
+    ncpu = os.cpu_count() or 1
+    procs = max(1, min(ncpu, args.ref_procs or ncpu))
+    res = cpu_reference(args, procs, 1, args.steps, args.warmup, w)
+    value = res["value"]
+    ms = 1e3 * sum(res["step_s"]) / len(res["step_s"])
+    line = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded uniform charges and positions)",
+        "config": {"workload": workload_name(dict(w, precision="fp64")) + " (CPU reference)",
+                   "N": w["N"], "M": w["M"], "P": w["P"], "xi": w["xi"]},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "particles/s", "cores": res["cores"],
+                         "kind": res["kind"], "sample": res["sample"]},
+        "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-procs", type=int, default=0,
+                    help="CPU processes for --impl reference (default: all cores)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from se_fast_gridding_b200 import solver
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+    w = WORKLOAD
+    N = w["N"]
+    import oracle as O   # seeded inputs and the accuracy check (checker only)
+    x_np, q_np = O.synthetic_system(N, w["L"], seed=w["seed"] + rank, charges=w["charges"])
+    m = solver.default_m(w["P"])
+    se = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], w["precision"], N)
+    x = torch.tensor(x_np, device=dev)
+    q = torch.tensor(q_np, device=dev)
+    out = torch.empty(3 * N, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # accuracy (rank 0, outside the timed region): FP32 vs the FP64 path and
+    # vs the FP64 direct k-space sum on the 1,000-particle subset
+    accuracy = None
+    if rank == 0:
+        se.solve(x, q, out)
+        f32 = out.cpu().numpy()
+        s64 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp64", N)
+        f64 = s64.solve(x, q).cpu().numpy()
+        s64.close()
+        accuracy = {"rel_rms_fp32_vs_fp64": O.rel_rms(f32, f64)}
+        gpath = os.path.join(ROOT, "tests", "golden", "c2.npz")
+        if os.path.exists(gpath):
+            g = np.load(gpath)
+            t = g["targets"]
+            sub = np.concatenate([f32[t + d * N] for d in range(3)])
+            accuracy["rel_rms_vs_direct_1000"] = O.rel_rms(sub, g["force_direct"])
+            sub64 = np.concatenate([f64[t + d * N] for d in range(3)])
+            accuracy["rel_rms_fp64_vs_direct_1000"] = O.rel_rms(sub64, g["force_direct"])
+
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    se.set_timing(True)
+    for _ in range(args.warmup):
+        flush.fill_(1.0)
+        se.solve(x, q, out)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    stage = {"sort": [], "spread": [], "kspace": [], "interp": []}
+    launches = 0
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        se.solve(x, q, out)
+        ev[k][1].record(stream)
+        launches += se.launches
+        for key, v in se.stage_ms().items():
+            stage[key].append(v)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    ms = sum(step_ms) / len(step_ms)
+    clk = clocks.stop()
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    value = world * N / (ms * 1e-3)
+    stage_avg = {k: sum(v) / len(v) for k, v in stage.items()}
+
+    # end to end through the host-buffer entry point, pinned buffers
+    xh = torch.tensor(x_np).pin_memory()
+    qh = torch.tensor(q_np).pin_memory()
+    oh = torch.empty(3 * N, dtype=torch.float64).pin_memory()
+    se.set_timing(False)
+    for _ in range(max(args.warmup, 1)):
+        se.solve_host_ptr(N, xh.data_ptr(), qh.data_ptr(), oh.data_ptr())
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        se.solve_host_ptr(N, xh.data_ptr(), qh.data_ptr(), oh.data_ptr())
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e = sum(e2e_ms) / len(e2e_ms)
+    if pg:
+        t = torch.tensor([e2e], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e = float(t.item())
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel
+    hbm, hbm_kind = measured_peaks()
+    fma = solver.fma_peak_tflops()
+    s = 4 if w["precision"] == "fp32" else 8
+    P, M = w["P"], w["M"]
+    dom = max(("spread", "interp"), key=lambda k: stage_avg[k])
+    if dom == "spread":
+        alg_bytes = N * 4 * 8 + M ** 3 * 8      # x, q in; M^3 FP64 grid out
+        flops = 2.0 * P ** 3 * N
+    else:
+        alg_bytes = M ** 3 * 8 + N * 4 * 8 + 3 * N * 8
+        flops = 8.0 * P ** 3 * N
+    t_dom = stage_avg[dom] * 1e-3
+    tr = ncu_traffic()
+    traffic = None
+    if tr and tr.get("workload") == workload_name(w):
+        traffic = tr.get(dom)
+    roofline = {"kernel": f"k_{dom}", "bound": "hbm", "achieved": alg_bytes / t_dom / 1e9,
+                "peak": hbm, "unit": "GB/s", "frac": alg_bytes / t_dom / 1e9 / hbm,
+                "traffic": traffic, "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                if hbm_kind == "measured" else "fallback 6650 GB/s",
+                "algorithmic_bytes": alg_bytes}
+    roofline_fma = {"kernel": f"k_{dom}", "bound": "fp32_fma", "achieved": flops / t_dom / 1e12,
+                    "peak": fma, "unit": "TFLOP/s", "frac": flops / t_dom / 1e12 / fma,
+                    "peak_source": "measured FMA-chain kernel (se_probe_fma_tflops)"}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            res = cpu_reference(args, 1, 1, 1, 0, w)
+            cpu = {"value": res["value"], "unit": "particles/s", "cores": res["cores"],
+                   "kind": res["kind"], "sample": res["sample"]}
+        except Exception as e:   # the baseline is reported, not required
+            cpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference",
+                   "sample": f"failed: {e}"[:200]}
+    line = {
+        "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform charges and positions, one replica per GPU)",
+        "config": {"workload": workload_name(w), "N": N, "M": M, "P": P, "xi": w["xi"],
+                   "L": w["L"], "precision": w["precision"], "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "roofline": roofline, "roofline_fma": roofline_fma,
+        "stage_ms": stage_avg, "cpu_baseline": cpu,
+        "e2e": {"value": world * N / (e2e * 1e-3), "unit": "particles/s",
+                "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 3 * N * 8,
+                "ms_per_step": e2e},
+        "gpu_launches": launches,
+        "clocks": clk, "accuracy": accuracy, "wall_s_timed": wall,
+    }
+    print(json.dumps(line), flush=True)
+    se.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * se_gpu.h -- device-resident API of libse_gpu.so (B200, sm_100a).
+ *
+ * One plan holds everything a Spectral Ewald k-space solve of one cubic,
+ * three-periodic system needs on the GPU: the sorted particle records, the
+ * M^3 periodic grid, the half spectrum, the cuFFT plans.  se_solve() runs the
+ * path of spectral_ewald.c:20-182 (SE_fast_gridding) with no host round trip:
+ *
+ *   prepare -> stable counting sort by grid bin -> spread with the periodic
+ *   fold fused (SE_FGG_grid + SE_FGG_wrap_fcn) -> cuFFT D2Z -> Green's
+ *   function scaling (scaling/product_rc, SE_general.c:145-175,336-362) ->
+ *   cuFFT Z2D -> interpolation with the periodic unfold fused (SE_FGG_extend_fcn
+ *   + SE_FGG_int / SE_FGG_int_force)
+ *
+ * Parameters follow parse_params / SE_FGG_FCN_params (SE_general.c:16-29,
+ * 180-200): h = L/M, w = P h/2, eta = (2 w xi/m)^2, c = 2 xi^2/eta,
+ * d = (c/pi)^{3/2}.  Positions are SoA (x[n], x[n+N], x[n+2N]) in FP64 as in
+ * the reference; FORCE output is SoA with the reference's convention
+ * F = h^3 q sum H W (-c)(x - x_grid) (SE_fgg.c:1024-1100).
+ *
+ * Precision SE_FP64 matches the reference's FP64 CPU path to ~1e-13 relative.
+ * SE_FP32 spreads and interpolates in FP32 with compensated (per-chunk FP32,
+ * cross-chunk FP64) accumulation; the FFT, the scaling and the energy stay
+ * FP64.
+ *
+ * All functions return 0 (SE_OK) or an SE_ERR_* code; pointers are device
+ * pointers unless the name ends in _host; streams are cudaStream_t passed as
+ * void* (NULL = the legacy default stream).  A plan may be used by one stream
+ * at a time.
+ */
+#ifndef SE_GPU_H
+#define SE_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SE_OK = 0,
+    SE_ERR_CUDA = 1,
+    SE_ERR_INVALID = 2,
+    SE_ERR_UNSUPPORTED = 3,
+    SE_ERR_NOMEM = 4,
+    SE_ERR_CUFFT = 5,
+    SE_ERR_INPUT = 6     /* a position was not finite */
+};
+
+enum { SE_POTENTIAL = 0, SE_FORCE = 1 };
+enum { SE_FP64 = 0, SE_FP32 = 1 };
+
+typedef struct {
+    int M;              /* grid points per dimension (cubic grid)              */
+    int P;              /* Gaussian support, 1 <= P <= 32                     */
+    double L;           /* box side                                           */
+    double xi;          /* Ewald parameter                                    */
+    double m;           /* Gaussian shape factor                              */
+    int mode;           /* SE_POTENTIAL or SE_FORCE                           */
+    int precision;      /* SE_FP64 or SE_FP32                                 */
+    int max_particles;  /* capacity of the plan                               */
+} se_config;
+
+typedef struct se_plan_s* se_plan;
+
+/* Derived FGG parameters of a configuration (no GPU needed). */
+int se_config_derive(const se_config* cfg, double* h, double* w, double* eta,
+                     double* c, double* d);
+
+/* Device bytes a plan of this configuration holds (admission control). */
+size_t se_plan_device_bytes(const se_config* cfg);
+
+int se_plan_create(se_plan* plan, const se_config* cfg);
+int se_plan_destroy(se_plan plan);
+
+/* Full k-space solve on device buffers.  out: N (POTENTIAL) or 3N (FORCE).
+ * phi_out (may be NULL) additionally receives the potential in FORCE mode. */
+int se_solve(se_plan plan, int N, const double* x, const double* q, double* out,
+             double* phi_out, void* stream);
+
+/* The same through host buffers: copies in, solves, copies out, waits. */
+int se_solve_host(se_plan plan, int N, const double* x_host, const double* q_host,
+                  double* out_host, void* stream);
+
+/* The steps, for callers that want the intermediate grid.
+ * grid: M^3 FP64, row-major [x][y][z] (the transpose of the column-major
+ * H_per of SE_FGG_wrap_fcn). */
+int se_spread(se_plan plan, int N, const double* x, const double* q, double* grid,
+              void* stream);
+int se_kspace(se_plan plan, double* grid, void* stream);
+int se_interp(se_plan plan, int N, const double* x, const double* q, const double* grid,
+              double* out, double* phi_out, void* stream);
+
+/* E = 1/2 sum phi q (calc_energy, SE_fgg.c:5934-5946), FP64, deterministic. */
+int se_energy(const double* phi, const double* q, int N, double* energy_dev, void* stream);
+
+/* Kernel launches the last se_solve() on this plan issued (for accounting). */
+int se_plan_launch_count(se_plan plan);
+
+/* Text of the last CUDA / cuFFT failure seen on this thread. */
+const char* se_gpu_error_detail(void);
+
+/* Per-stage timing: with timing on, each solve records CUDA events on its
+ * stream; se_plan_stage_ms waits for the last solve and returns the
+ * milliseconds of [prepare+sort, spread, k-space (FFT, scaling, FFT), interp]. */
+int se_plan_set_timing(se_plan plan, int on);
+int se_plan_stage_ms(se_plan plan, float ms[4]);
+
+/* FP32 FMA throughput (TFLOP/s) of the current GPU from an FMA-chain kernel:
+ * the compute roofline of the spread and interpolation kernels. */
+int se_probe_fma_tflops(double* tflops, void* stream);
+
+/* Stable counting sort of N keys in [0, nkeys): perm[s] = input index of the
+ * s-th smallest key, ties in input order; offsets[nkeys+1] bin starts.
+ * Device buffers; scratch from se_sort_scratch_bytes(). */
+size_t se_sort_scratch_bytes(int N, int nkeys);
+int se_counting_sort(const int* keys, int N, int nkeys, int* perm, int* offsets,
+                     void* scratch, size_t scratch_bytes, void* stream);
+
+/* ---------------------------------------------------------------- batch -- */
+/* Many independent systems solved together: one sort, one spread launch and
+ * one interpolation launch over all systems through per-system offset
+ * tables, and one batched cuFFT plan per distinct grid size. */
+typedef struct {
+    int N;
+    int M;
+    int P;
+    double L;
+    double xi;
+    double m;
+    int mode;           /* SE_POTENTIAL or SE_FORCE */
+} se_system;
+
+typedef struct se_batch_s* se_batch;
+
+int se_batch_create(se_batch* batch, const se_system* systems, int nsys, int precision);
+int se_batch_destroy(se_batch batch);
+size_t se_batch_device_bytes(const se_system* systems, int nsys, int precision);
+/* x: concatenated per-system SoA blocks (3 N_s each), q: concatenated N_s,
+ * out: concatenated N_s (POTENTIAL) or 3 N_s (FORCE) blocks. */
+int se_batch_solve(se_batch batch, const double* x, const double* q, double* out,
+                   void* stream);
+int se_batch_launch_count(se_batch batch);
+int se_batch_set_timing(se_batch batch, int on);
+int se_batch_stage_ms(se_batch batch, float ms[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SE_GPU_H */

@@ -1,0 +1,1281 @@
+// se_solve.cu -- device-resident Spectral Ewald k-space solve on B200.
+//
+// One launch of each step covers every system of a batch (a single-system
+// plan is a batch of one); per-system parameters and offsets live in a small
+// device table (SysDev).
+//
+//   k_prepare   per particle: stencil corner and offset as fgg_expansion_3p
+//               (SE_fgg.c:539-621), charge x d, fine-bin key
+//   stable_sort by fine-bin key (se_sort.cu), then k_gather into bin order
+//   k_spread    one CTA per output tile of the periodic grid: every particle
+//               whose stencil reaches the tile contributes through per-tile
+//               separable factor rows built with the FGG recurrence
+//               exp(-c u^2), r = exp(2chu - ch^2), r <- r exp(-2ch^2); cells
+//               accumulate in registers and are written once, so the periodic
+//               fold of SE_FGG_wrap_fcn (SE_fgg.c:327-352) needs no atomics
+//   cuFFT D2Z, k_scale (Z of scaling(), SE_general.c:145-175, applied to the
+//               half spectrum as product_rc does, SE_general.c:336-362), Z2D
+//   k_interp    one CTA per fine bin: the bin's (8+P-1)^3 window of the
+//               periodic grid is staged in shared memory (the unfold of
+//               SE_FGG_extend_fcn, SE_fgg.c:417-443), one warp per particle
+//               gathers sum H W (SE_fgg.c:968-1100)
+//
+// Grid layout: M^3 FP64 row-major [x][y][z], the transpose of the reference's
+// column-major H_per; the FFT of the transpose is the transpose of the FFT and
+// Z is symmetric in the axes, so results are identical.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "se_internal.h"
+
+namespace se {
+
+// --------------------------------------------------------------- errors ---
+
+static thread_local char g_err_msg[256];
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line)
+{
+    snprintf(g_err_msg, sizeof(g_err_msg), "%s:%d %s: %s", file, line, what,
+             cudaGetErrorString(e));
+    fprintf(stderr, "[se_gpu] %s\n", g_err_msg);
+    return e == cudaErrorMemoryAllocation ? SE_ERR_NOMEM : SE_ERR_CUDA;
+}
+
+static int cufft_fail(cufftResult r, const char* what)
+{
+    snprintf(g_err_msg, sizeof(g_err_msg), "cuFFT %s failed (%d)", what, (int)r);
+    fprintf(stderr, "[se_gpu] %s\n", g_err_msg);
+    return r == CUFFT_ALLOC_FAILED ? SE_ERR_NOMEM : SE_ERR_CUFFT;
+}
+
+#define SE_CUFFT(call)                                                        \
+    do {                                                                      \
+        cufftResult se_r_ = (call);                                           \
+        if (se_r_ != CUFFT_SUCCESS) return cufft_fail(se_r_, #call);          \
+    } while (0)
+
+// ----------------------------------------------------------- geometry -----
+
+constexpr int FB = 8;                     // fine bin edge, in stencil corners
+constexpr int TX = 8, TY = 16, TZ = 16;   // spread tile (output cells)
+constexpr int SPREAD_THREADS = 128;
+constexpr int CHUNK = 64;                 // particles staged per spread round
+constexpr int INTERP_WARPS = 8;
+constexpr int MAX_P = 32;
+constexpr double PI_D = 3.14159265358979323846;
+
+struct SysDev {
+    int N, M, P, lo, mode;
+    int part_off, out_off;
+    long long grid_off, spec_off;
+    int nf[3];
+    int bin_base;
+    int nt[3];
+    int tile_base;
+    double h, c, d, h3;
+    double rho;      // exp(-2 c h^2)
+    double kfac;     // 2 pi / L
+    double scalar;   // -(1 - eta) / (4 xi^2)
+    double dnorm;    // 4 pi / M^3
+};
+
+__device__ __forceinline__ int find_sys(const int* __restrict__ prefix, int nsys, int v)
+{
+    // largest s with prefix[s] <= v
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int pmod(int i, int n)
+{
+    const int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ int pack_g(int gx, int gy, int gz) { return gx | (gy << 10) | (gz << 20); }
+__device__ __forceinline__ int g_of(int pk, int a) { return (pk >> (10 * a)) & 1023; }
+
+// --------------------------------------------------------------- prepare --
+
+__global__ void k_prepare(const SysDev* __restrict__ sys, const int* __restrict__ part_prefix,
+                          int nsys, int ntot, const double* __restrict__ x,
+                          const double* __restrict__ q, int* __restrict__ key,
+                          double4* __restrict__ rec, int* __restrict__ gpk, int* err)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ntot) return;
+    const int s = find_sys(part_prefix, nsys, n);
+    const SysDev& S = sys[s];
+    const int i = n - S.part_off;
+    const double* xs = x + 3LL * S.part_off;
+    const bool odd = S.P & 1;
+    double t0[3];
+    int g[3];
+    bool ok = true;
+    for (int a = 0; a < 3; a++) {
+        const double xa = xs[i + (long long)a * S.N];
+        const double u = xa / S.h;
+        if (!(fabs(u) < 1.0e9)) {   // NaN / Inf / absurd positions
+            ok = false;
+            t0[a] = 0.0;
+            g[a] = 0;
+            continue;
+        }
+        const int cell = odd ? (int)round(u) : (int)floor(u);
+        t0[a] = xa - S.h * cell;
+        g[a] = pmod(cell + S.lo, S.M);
+    }
+    if (!ok) atomicOr(err, 1);
+    const double qw = ok ? q[S.part_off + i] * S.d : 0.0;
+    rec[n] = make_double4(t0[0], t0[1], t0[2], qw);
+    gpk[n] = pack_g(g[0], g[1], g[2]);
+    key[n] = S.bin_base + ((g[0] / FB) * S.nf[1] + g[1] / FB) * S.nf[2] + g[2] / FB;
+}
+
+__global__ void k_gather(int ntot, const int* __restrict__ perm, const double4* __restrict__ rec,
+                         const int* __restrict__ gpk, double4* __restrict__ srec,
+                         int* __restrict__ sg)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ntot) return;
+    const int j = perm[s];
+    srec[s] = rec[j];
+    sg[s] = gpk[j];
+}
+
+// ------------------------------------------------------- factor rows -----
+
+// Gaussian factors exp(-c (t0 - (lo+i) h)^2) for the T cells o..o+T-1 of one
+// axis, i = (cell - g) mod M, zero where i >= P or the cell is outside [0, M).
+// Runs of consecutive i use the FGG recurrence (two exps per run).  Returns a
+// bitmask of the nonzero entries.
+template <int T, typename Acc>
+__device__ __forceinline__ unsigned factor_row(Acc* out, int o, int g, double t0, double scale,
+                                               const SysDev& S)
+{
+    unsigned mask = 0;
+    int i = pmod(o - g, S.M);
+    double v = 0.0, r = 0.0;
+    int prev = -2;
+#pragma unroll
+    for (int xo = 0; xo < T; xo++) {
+        double val = 0.0;
+        if (o + xo < S.M && i < S.P) {
+            if (i == prev + 1) {
+                v *= r;
+                r *= S.rho;
+            } else {
+                const double u = t0 - (S.lo + i) * S.h;
+                v = exp(-S.c * u * u);
+                r = exp(2.0 * S.c * S.h * u - S.c * S.h * S.h);
+            }
+            prev = i;
+            val = v * scale;
+            mask |= 1u << xo;
+        } else {
+            prev = -2;
+        }
+        out[xo] = (Acc)val;
+        if (++i == S.M) i = 0;
+    }
+    return mask;
+}
+
+// ---------------------------------------------------------------- spread --
+
+// Up to two fine-bin ranges whose corners reach the output cells [o, o+T).
+struct BinRanges {
+    int a0, a1, b0, b1;   // [a0,a1] and [b0,b1], b0 > b1 when absent
+};
+
+__device__ __forceinline__ BinRanges bins_reaching(int o, int T, int M, int P, int nf)
+{
+    BinRanges r;
+    const int Ta = min(T, M - o);
+    const int len = Ta + P - 1;   // corners g with (g + i) mod M in the tile, i < P
+    if (len >= M) {
+        r.a0 = 0; r.a1 = nf - 1; r.b0 = 1; r.b1 = 0;
+        return r;
+    }
+    const int start = pmod(o - P + 1, M);
+    const int end = start + len - 1;
+    if (end < M) {
+        r.a0 = start / FB; r.a1 = end / FB; r.b0 = 1; r.b1 = 0;
+    } else {
+        const int e2 = end - M;
+        r.a0 = start / FB; r.a1 = nf - 1;
+        r.b0 = 0; r.b1 = e2 / FB;
+        if (r.b1 >= r.a0) { r.a0 = 0; r.a1 = nf - 1; r.b0 = 1; r.b1 = 0; }
+    }
+    return r;
+}
+
+template <typename Acc>
+struct SpreadSmem {
+    Acc px[CHUNK][TX];
+    Acc py[CHUNK][TY];
+    Acc pz[CHUNK][TZ];
+    unsigned ymask[CHUNK];
+};
+
+template <typename Acc>
+__device__ __forceinline__ void spread_chunk(const SysDev& S, SpreadSmem<Acc>& sm,
+                                             const double4* __restrict__ srec,
+                                             const int* __restrict__ sg, int c0, int n, int x0,
+                                             int y0, int z0, Acc (&acc)[4][4], int xh, int z4,
+                                             int yy)
+{
+    __syncthreads();   // the previous chunk's rows are consumed
+    for (int u = threadIdx.x; u < n * 3; u += SPREAD_THREADS) {
+        const int p = u / 3, a = u - 3 * (u / 3);
+        const double4 rc = srec[c0 + p];
+        const int pk = sg[c0 + p];
+        if (a == 0) factor_row<TX, Acc>(sm.px[p], x0, g_of(pk, 0), rc.x, rc.w, S);
+        else if (a == 1) sm.ymask[p] = factor_row<TY, Acc>(sm.py[p], y0, g_of(pk, 1), rc.y, 1.0, S);
+        else factor_row<TZ, Acc>(sm.pz[p], z0, g_of(pk, 2), rc.z, 1.0, S);
+    }
+    __syncthreads();
+    const int wrow = yy & ~3;   // the 4 rows of this warp
+    for (int p = 0; p < n; p++) {
+        if (((sm.ymask[p] >> wrow) & 0xFu) == 0u) continue;   // warp-uniform
+        const Acc wy = sm.py[p][yy];
+        Acc wz[4], wx[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            wz[k] = sm.pz[p][4 * z4 + k];
+            wx[k] = sm.px[p][4 * xh + k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const Acc cz = wy * wz[k];
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[j][k] = fma(wx[j], cz, acc[j][k]);
+        }
+    }
+}
+
+// One CTA per TX x TY x TZ tile of one system's periodic grid.  Thread t owns
+// the 4 x 4 cells (x0 + 4 xh + j, y0 + yy, z0 + 4 z4 + k).
+template <typename Acc>
+__global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
+    const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
+    const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ boff, double* __restrict__ grid)
+{
+    __shared__ __align__(16) SpreadSmem<Acc> sm;
+    const int tile = blockIdx.x;
+    const int s = find_sys(tile_prefix, nsys, tile);
+    const SysDev& S = sys[s];
+    const int lt = tile - S.tile_base;
+    const int ax = lt / (S.nt[1] * S.nt[2]);
+    const int ay = (lt / S.nt[2]) % S.nt[1];
+    const int az = lt % S.nt[2];
+    const int x0 = ax * TX, y0 = ay * TY, z0 = az * TZ;
+    const int t = threadIdx.x;
+    const int xh = t & 1, z4 = (t >> 1) & 3, yy = t >> 3;
+
+    Acc acc[4][4];
+    double accd[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) { acc[j][k] = Acc(0); accd[j][k] = 0.0; }
+
+    const BinRanges rx = bins_reaching(x0, TX, S.M, S.P, S.nf[0]);
+    const BinRanges ry = bins_reaching(y0, TY, S.M, S.P, S.nf[1]);
+    const BinRanges rz = bins_reaching(z0, TZ, S.M, S.P, S.nf[2]);
+    for (int ix = 0; ix < 2; ix++) {
+        const int bx0 = ix ? rx.b0 : rx.a0, bx1 = ix ? rx.b1 : rx.a1;
+        for (int bx = bx0; bx <= bx1; bx++)
+            for (int iy = 0; iy < 2; iy++) {
+                const int by0 = iy ? ry.b0 : ry.a0, by1 = iy ? ry.b1 : ry.a1;
+                for (int by = by0; by <= by1; by++)
+                    for (int iz = 0; iz < 2; iz++) {
+                        const int bz0 = iz ? rz.b0 : rz.a0, bz1 = iz ? rz.b1 : rz.a1;
+                        if (bz0 > bz1) continue;
+                        const int kb = S.bin_base + (bx * S.nf[1] + by) * S.nf[2];
+                        const int beg = boff[kb + bz0], end = boff[kb + bz1 + 1];
+                        for (int c0 = beg; c0 < end; c0 += CHUNK) {
+                            spread_chunk<Acc>(S, sm, srec, sg, c0, min(CHUNK, end - c0), x0,
+                                              y0, z0, acc, xh, z4, yy);
+                            if (sizeof(Acc) == 4) {   // compensated: fold the chunk sum
+#pragma unroll
+                                for (int j = 0; j < 4; j++)
+#pragma unroll
+                                    for (int k = 0; k < 4; k++) {
+                                        accd[j][k] += (double)acc[j][k];
+                                        acc[j][k] = Acc(0);
+                                    }
+                            }
+                        }
+                    }
+            }
+    }
+    const int gy = y0 + yy;
+    if (gy >= S.M) return;
+    double* gs = grid + S.grid_off;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int gx = x0 + 4 * xh + j;
+        if (gx >= S.M) continue;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int gz = z0 + 4 * z4 + k;
+            if (gz < S.M)
+                gs[((long long)gx * S.M + gy) * S.M + gz] =
+                    sizeof(Acc) == 4 ? accd[j][k] : (double)acc[j][k];
+        }
+    }
+}
+
+// --------------------------------------------------------------- k-space --
+
+__device__ __forceinline__ double kwave(int i, int M, double kfac)
+{
+    const int npos = (M % 2 == 0) ? M / 2 : (M - 1) / 2 + 1;
+    return kfac * (double)(i < npos ? i : i - M);
+}
+
+// spec *= Z on the half spectrum [x][y][z <= M/2]; Z = exp(scalar K2)/K2 * 4pi/M^3
+// with K2 summed in the reference's order (its first FFT axis is our z).
+__global__ void k_scale(const SysDev* __restrict__ sys, double2* __restrict__ spec)
+{
+    const SysDev& S = sys[blockIdx.y];
+    const int M = S.M, Mh = M / 2 + 1;
+    const long long n = (long long)M * M * Mh;
+    double2* sp = spec + S.spec_off;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int iz = (int)(e % Mh);
+        const int iy = (int)((e / Mh) % M);
+        const int ix = (int)(e / ((long long)Mh * M));
+        const double kx = kwave(ix, M, S.kfac), ky = kwave(iy, M, S.kfac),
+                     kz = kwave(iz, M, S.kfac);
+        const double K2 = (kz * kz + ky * ky) + kx * kx;
+        const double Z = (e == 0) ? 0.0 : exp(S.scalar * K2) / K2 * S.dnorm;
+        double2 v = sp[e];
+        v.x *= Z;
+        v.y *= Z;
+        sp[e] = v;
+    }
+}
+
+// ---------------------------------------------------------------- interp --
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct InterpWarpSmem {
+    double w[3][MAX_P];    // Gaussian factors per axis
+    double wf[3][MAX_P];   // times -c u (force)
+};
+
+// One CTA per fine bin; E = FB + P - 1 cells per axis staged (pitch E|1).
+// PT = P at compile time (0: runtime P).
+template <typename T, int PT>
+__global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
+    const SysDev* __restrict__ sys, const int* __restrict__ bin_prefix, int nsys,
+    const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ sperm, const int* __restrict__ boff,
+    const double* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ InterpWarpSmem wsm[INTERP_WARPS];
+    const int bin = blockIdx.x;
+    const int beg = boff[bin], end = boff[bin + 1];
+    if (beg == end) return;
+    const int s = find_sys(bin_prefix, nsys, bin);
+    const SysDev& S = sys[s];
+    const int P = PT ? PT : S.P;
+    const int M = S.M;
+    const int lb = bin - S.bin_base;
+    const int o[3] = {(lb / (S.nf[1] * S.nf[2])) * FB, ((lb / S.nf[2]) % S.nf[1]) * FB,
+                      (lb % S.nf[2]) * FB};
+    const int E = FB + P - 1, Ep = E | 1;
+    T* tile = reinterpret_cast<T*>(dsm);
+    const double* gs = grid + S.grid_off;
+    // stage the periodic window [o, o + E) mod M
+    for (int e = threadIdx.x; e < E * E * E; e += blockDim.x) {
+        const int c = e % E, b = (e / E) % E, a = e / (E * E);
+        const int gx = pmod(o[0] + a, M), gy = pmod(o[1] + b, M), gz = pmod(o[2] + c, M);
+        tile[(a * E + b) * Ep + c] = (T)gs[((long long)gx * M + gy) * M + gz];
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    InterpWarpSmem& W = wsm[warp];
+    const bool force = S.mode == SE_FORCE;
+    for (int p = beg + warp; p < end; p += INTERP_WARPS) {
+        const double4 rc = srec[p];
+        const int pk = sg[p];
+        const int r0 = g_of(pk, 0) - o[0], r1 = g_of(pk, 1) - o[1], r2 = g_of(pk, 2) - o[2];
+        if (lane < P) {
+            const double t0[3] = {rc.x, rc.y, rc.z};
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const double u = t0[a] - (S.lo + lane) * S.h;
+                const double v = exp(-S.c * u * u);
+                W.w[a][lane] = v;
+                W.wf[a][lane] = v * (-S.c * u);
+            }
+        }
+        __syncwarp();
+        T wz[PT ? PT : MAX_P], wzf[PT ? PT : MAX_P];
+        if (PT) {
+#pragma unroll
+            for (int k = 0; k < (PT ? PT : 1); k++) {
+                wz[k] = (T)W.w[2][k];
+                wzf[k] = (T)W.wf[2][k];
+            }
+        }
+        double a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
+        for (int r = lane; r < P * P; r += 32) {
+            const int i = r / P, j = r - (r / P) * P;
+            const T* row = tile + ((r0 + i) * E + (r1 + j)) * Ep + r2;
+            T s0 = 0, s1 = 0;
+            if (PT) {
+#pragma unroll
+                for (int k = 0; k < (PT ? PT : 1); k++) {
+                    const T hv = row[k];
+                    s0 = fma(hv, wz[k], s0);
+                    if (force) s1 = fma(hv, wzf[k], s1);
+                }
+            } else {
+                for (int k = 0; k < P; k++) {
+                    const T hv = row[k];
+                    s0 = fma(hv, (T)W.w[2][k], s0);
+                    if (force) s1 = fma(hv, (T)W.wf[2][k], s1);
+                }
+            }
+            const double wxi = W.w[0][i], wyj = W.w[1][j];
+            a_pot = fma((double)s0, wxi * wyj, a_pot);
+            if (force) {
+                a_fx = fma((double)s0, W.wf[0][i] * wyj, a_fx);
+                a_fy = fma((double)s0, wxi * W.wf[1][j], a_fy);
+                a_fz = fma((double)s1, wxi * wyj, a_fz);
+            }
+        }
+        a_pot = warp_sum(a_pot);
+        if (force) {
+            a_fx = warp_sum(a_fx);
+            a_fy = warp_sum(a_fy);
+            a_fz = warp_sum(a_fz);
+        }
+        if (lane == 0) {
+            const int loc = sperm[p] - S.part_off;
+            const double scale = S.h3 * S.d;
+            if (force) {
+                const double qs = rc.w / S.d * scale;   // q h^3 d
+                out[S.out_off + loc] = qs * a_fx;
+                out[S.out_off + loc + S.N] = qs * a_fy;
+                out[S.out_off + loc + 2 * S.N] = qs * a_fz;
+                if (phi_out) phi_out[S.part_off + loc] = scale * a_pot;
+            } else {
+                out[S.out_off + loc] = scale * a_pot;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Interpolation without staging, for windows that exceed shared memory
+// (large P in FP64): the same sums read from the periodic grid in L2.
+__global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp_global(
+    const SysDev* __restrict__ sys, const int* __restrict__ part_prefix, int nsys, int ntot,
+    const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ sperm, const double* __restrict__ grid, double* __restrict__ out,
+    double* __restrict__ phi_out)
+{
+    __shared__ InterpWarpSmem wsm[INTERP_WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = blockIdx.x * INTERP_WARPS + warp;
+    if (p >= ntot) return;
+    const int orig = sperm[p];
+    const int s = find_sys(part_prefix, nsys, orig);
+    const SysDev& S = sys[s];
+    const int P = S.P, M = S.M;
+    InterpWarpSmem& W = wsm[warp];
+    const double4 rc = srec[p];
+    const int pk = sg[p];
+    const int g0 = g_of(pk, 0), g1 = g_of(pk, 1), g2 = g_of(pk, 2);
+    if (lane < P) {
+        const double t0[3] = {rc.x, rc.y, rc.z};
+        for (int a = 0; a < 3; a++) {
+            const double u = t0[a] - (S.lo + lane) * S.h;
+            const double v = exp(-S.c * u * u);
+            W.w[a][lane] = v;
+            W.wf[a][lane] = v * (-S.c * u);
+        }
+    }
+    __syncwarp();
+    const bool force = S.mode == SE_FORCE;
+    const double* gs = grid + S.grid_off;
+    double a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
+    for (int r = lane; r < P * P; r += 32) {
+        const int i = r / P, j = r % P;
+        const double* row = gs + ((long long)pmod(g0 + i, M) * M + pmod(g1 + j, M)) * M;
+        double s0 = 0, s1 = 0;
+        int z = g2;
+        for (int k = 0; k < P; k++) {
+            const double hv = __ldg(row + z);
+            s0 = fma(hv, W.w[2][k], s0);
+            if (force) s1 = fma(hv, W.wf[2][k], s1);
+            if (++z == M) z = 0;
+        }
+        const double wxi = W.w[0][i], wyj = W.w[1][j];
+        a_pot = fma(s0, wxi * wyj, a_pot);
+        if (force) {
+            a_fx = fma(s0, W.wf[0][i] * wyj, a_fx);
+            a_fy = fma(s0, wxi * W.wf[1][j], a_fy);
+            a_fz = fma(s1, wxi * wyj, a_fz);
+        }
+    }
+    a_pot = warp_sum(a_pot);
+    if (force) {
+        a_fx = warp_sum(a_fx);
+        a_fy = warp_sum(a_fy);
+        a_fz = warp_sum(a_fz);
+    }
+    if (lane == 0) {
+        const int loc = orig - S.part_off;
+        const double scale = S.h3 * S.d;
+        if (force) {
+            const double qs = rc.w / S.d * scale;
+            out[S.out_off + loc] = qs * a_fx;
+            out[S.out_off + loc + S.N] = qs * a_fy;
+            out[S.out_off + loc + 2 * S.N] = qs * a_fz;
+            if (phi_out) phi_out[S.part_off + loc] = scale * a_pot;
+        } else {
+            out[S.out_off + loc] = scale * a_pot;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- energy --
+
+__global__ void k_energy_partial(const double* __restrict__ phi, const double* __restrict__ q,
+                                 int N, double* __restrict__ partial)
+{
+    __shared__ double ws[32];
+    double s = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (long long)gridDim.x * blockDim.x)
+        s += phi[i] * q[i];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < blockDim.x / 32 ? ws[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) partial[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_energy_final(const double* __restrict__ partial, int n, double* e)
+{
+    __shared__ double ws[32];
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < blockDim.x / 32 ? ws[threadIdx.x] : 0.0;
+        v = warp_sum(v);
+        if (threadIdx.x == 0) *e = v / 2.;
+    }
+}
+
+// ---------------------------------------------------------------- batch ---
+
+struct HostSys {
+    se_system d;
+};
+
+struct FftGroup {
+    int M, count;
+    long long grid_off, spec_off;
+    cufftHandle fwd, bwd;
+};
+
+}  // namespace se
+
+struct se_batch_s {
+    int nsys = 0, precision = SE_FP64;
+    int ntot = 0, nbins = 0, ntiles = 0;
+    long long grid_elems = 0, spec_elems = 0;
+    std::vector<se::SysDev> host_sys;
+    std::vector<int> part_prefix, tile_prefix, bin_prefix;
+    std::vector<se::FftGroup> groups;
+    // device
+    se::SysDev* sys = nullptr;
+    int* d_part_prefix = nullptr;
+    int* d_tile_prefix = nullptr;
+    int* d_bin_prefix = nullptr;
+    int* key = nullptr;
+    double4* rec = nullptr;
+    int* gpk = nullptr;
+    int* perm = nullptr;
+    double4* srec = nullptr;
+    int* sg = nullptr;
+    int* boff = nullptr;
+    void* sort_scratch = nullptr;
+    size_t sort_bytes = 0;
+    double* grid = nullptr;
+    double2* spec = nullptr;
+    double* energy_partial = nullptr;
+    int* err = nullptr;
+    int launches = 0;
+    int max_P = 0;
+    bool staged_interp = true;
+    size_t interp_smem = 0;
+    // per-stage CUDA events (prepare+sort, spread, k-space, interp)
+    bool timing = false;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace se {
+
+static void derive(int M, int P, double L, double xi, double m, double* h, double* w,
+                   double* eta, double* c, double* d)
+{
+    // parse_params (SE_general.c:16-29), SE_FGG_FCN_params (SE_general.c:180-200)
+    const double h0 = L / (double)M;
+    const double w0 = (double)P * h0 / 2.;
+    const double r = 2.0 * w0 * xi / m;
+    const double eta0 = r * r;
+    const double c0 = 2.0 * xi * xi / eta0;
+    if (h) *h = L / M;
+    if (w) *w = w0;
+    if (eta) *eta = eta0;
+    if (c) *c = c0;
+    if (d) *d = pow(c0 / PI_D, 1.5);
+}
+
+static bool valid_system(const se_system& s)
+{
+    return s.N >= 0 && s.M >= 2 && s.M <= 1024 && s.P >= 1 && s.P <= MAX_P && s.P <= s.M &&
+           s.L > 0 && s.xi > 0 && s.m > 0 && (s.mode == SE_POTENTIAL || s.mode == SE_FORCE);
+}
+
+static size_t interp_smem_bytes(int P, int precision)
+{
+    const int E = FB + P - 1, Ep = E | 1;
+    return (size_t)E * E * Ep * (precision == SE_FP32 ? 4 : 8);
+}
+
+static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nbins_out,
+                          int* ntiles_out)
+{
+    long long ntot = 0, nbins = 0, ntiles = 0, grid = 0, spec = 0;
+    for (int i = 0; i < nsys; i++) {
+        const int M = sys[i].M;
+        const int nf = (M + FB - 1) / FB;
+        ntot += sys[i].N;
+        nbins += (long long)nf * nf * nf;
+        ntiles += (long long)((M + TX - 1) / TX) * ((M + TY - 1) / TY) * ((M + TZ - 1) / TZ);
+        grid += (long long)M * M * M;
+        spec += (long long)M * M * (M / 2 + 1);
+    }
+    if (nbins_out) *nbins_out = (int)nbins;
+    if (ntiles_out) *ntiles_out = (int)ntiles;
+    size_t b = 0;
+    b += (size_t)ntot * (4 + 32 + 4 + 4 + 32 + 4);
+    b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
+    b += (size_t)(nbins + 1) * 4;
+    b += (size_t)grid * 8 + (size_t)spec * 16;
+    // cuFFT work areas are about one spectrum more
+    b += (size_t)spec * 16;
+    b += (size_t)nsys * (sizeof(SysDev) + 12) + 4096;
+    return b;
+}
+
+static int batch_free(se_batch b)
+{
+    if (!b) return SE_OK;
+    for (auto& g : b->groups) {
+        if (g.fwd) cufftDestroy(g.fwd);
+        if (g.bwd) cufftDestroy(g.bwd);
+    }
+    for (auto& e : b->ev)
+        if (e) cudaEventDestroy(e);
+    void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
+                    b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
+                    b->grid, b->spec, b->energy_partial, b->err};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete b;
+    return SE_OK;
+}
+
+static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision)
+{
+    if (!out || !systems || nsys < 1 || (precision != SE_FP64 && precision != SE_FP32))
+        return SE_ERR_INVALID;
+    for (int i = 0; i < nsys; i++)
+        if (!valid_system(systems[i])) return SE_ERR_INVALID;
+    se_batch b = new se_batch_s();
+    b->nsys = nsys;
+    b->precision = precision;
+    // grids grouped by M (batched FFT plans need contiguous equal sizes)
+    std::vector<int> order(nsys);
+    for (int i = 0; i < nsys; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return systems[a].M < systems[c].M; });
+    std::vector<long long> goff(nsys), soff(nsys);
+    long long gcur = 0, scur = 0;
+    for (int k = 0; k < nsys; k++) {
+        const int i = order[k];
+        const int M = systems[i].M;
+        if (b->groups.empty() || b->groups.back().M != M) {
+            FftGroup g{};
+            g.M = M;
+            g.count = 0;
+            g.grid_off = gcur;
+            g.spec_off = scur;
+            b->groups.push_back(g);
+        }
+        b->groups.back().count++;
+        goff[i] = gcur;
+        soff[i] = scur;
+        gcur += (long long)M * M * M;
+        scur += (long long)M * M * (M / 2 + 1);
+    }
+    b->grid_elems = gcur;
+    b->spec_elems = scur;
+    int pcur = 0, ocur = 0, bcur = 0, tcur = 0;
+    b->host_sys.resize(nsys);
+    b->part_prefix.resize(nsys + 1);
+    b->tile_prefix.resize(nsys + 1);
+    b->bin_prefix.resize(nsys + 1);
+    for (int i = 0; i < nsys; i++) {
+        const se_system& s = systems[i];
+        SysDev& S = b->host_sys[i];
+        memset(&S, 0, sizeof(S));
+        double h, w, eta, c, d;
+        derive(s.M, s.P, s.L, s.xi, s.m, &h, &w, &eta, &c, &d);
+        const int ph = (s.P & 1) ? (s.P - 1) / 2 : s.P / 2;
+        S.N = s.N;
+        S.M = s.M;
+        S.P = s.P;
+        S.lo = (s.P & 1) ? -ph : -ph + 1;
+        S.mode = s.mode;
+        S.part_off = pcur;
+        S.out_off = ocur;
+        S.grid_off = goff[i];
+        S.spec_off = soff[i];
+        const int nf = (s.M + FB - 1) / FB;
+        S.nf[0] = S.nf[1] = S.nf[2] = nf;
+        S.bin_base = bcur;
+        S.nt[0] = (s.M + TX - 1) / TX;
+        S.nt[1] = (s.M + TY - 1) / TY;
+        S.nt[2] = (s.M + TZ - 1) / TZ;
+        S.tile_base = tcur;
+        S.h = h;
+        S.c = c;
+        S.d = d;
+        S.h3 = h * h * h;
+        S.rho = exp(-2.0 * c * h * h);
+        S.kfac = 2.0 * PI_D / s.L;
+        S.scalar = -(1. - eta) / (4. * s.xi * s.xi);
+        S.dnorm = 4. * PI_D / (double)(s.M * s.M * s.M);
+        b->part_prefix[i] = pcur;
+        b->tile_prefix[i] = tcur;
+        b->bin_prefix[i] = bcur;
+        pcur += s.N;
+        ocur += (s.mode == SE_FORCE ? 3 : 1) * s.N;
+        bcur += nf * nf * nf;
+        tcur += S.nt[0] * S.nt[1] * S.nt[2];
+        b->max_P = std::max(b->max_P, s.P);
+    }
+    b->part_prefix[nsys] = pcur;
+    b->tile_prefix[nsys] = tcur;
+    b->bin_prefix[nsys] = bcur;
+    b->ntot = pcur;
+    b->nbins = bcur;
+    b->ntiles = tcur;
+    b->interp_smem = interp_smem_bytes(b->max_P, precision);
+    b->staged_interp = b->interp_smem + sizeof(InterpWarpSmem) * INTERP_WARPS <= 220 * 1024;
+
+    auto fail = [&](int code) {
+        batch_free(b);
+        return code;
+    };
+#define SE_ALLOC(ptr, bytes)                                                    \
+    do {                                                                        \
+        cudaError_t e_ = cudaMalloc((void**)&(ptr), std::max<size_t>((bytes), 16)); \
+        if (e_ != cudaSuccess) return fail(cuda_fail(e_, "cudaMalloc", __FILE__, __LINE__)); \
+    } while (0)
+    const size_t nt = (size_t)std::max(b->ntot, 1);
+    SE_ALLOC(b->sys, sizeof(SysDev) * nsys);
+    SE_ALLOC(b->d_part_prefix, sizeof(int) * (nsys + 1));
+    SE_ALLOC(b->d_tile_prefix, sizeof(int) * (nsys + 1));
+    SE_ALLOC(b->d_bin_prefix, sizeof(int) * (nsys + 1));
+    SE_ALLOC(b->key, sizeof(int) * nt);
+    SE_ALLOC(b->rec, sizeof(double4) * nt);
+    SE_ALLOC(b->gpk, sizeof(int) * nt);
+    SE_ALLOC(b->perm, sizeof(int) * nt);
+    SE_ALLOC(b->srec, sizeof(double4) * nt);
+    SE_ALLOC(b->sg, sizeof(int) * nt);
+    SE_ALLOC(b->boff, sizeof(int) * (b->nbins + 1));
+    b->sort_bytes = sort_scratch_bytes(b->ntot, std::max(b->nbins, 1));
+    SE_ALLOC(b->sort_scratch, b->sort_bytes);
+    SE_ALLOC(b->grid, sizeof(double) * b->grid_elems);
+    SE_ALLOC(b->spec, sizeof(double2) * b->spec_elems);
+    SE_ALLOC(b->energy_partial, sizeof(double) * 1024);
+    SE_ALLOC(b->err, sizeof(int));
+#undef SE_ALLOC
+    cudaError_t e = cudaMemcpy(b->sys, b->host_sys.data(), sizeof(SysDev) * nsys,
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_part_prefix, b->part_prefix.data(), sizeof(int) * (nsys + 1),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_tile_prefix, b->tile_prefix.data(), sizeof(int) * (nsys + 1),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_bin_prefix, b->bin_prefix.data(), sizeof(int) * (nsys + 1),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(b->err, 0, sizeof(int));
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemcpy", __FILE__, __LINE__));
+    for (auto& g : b->groups) {
+        int n[3] = {g.M, g.M, g.M};
+        const int idist = g.M * g.M * g.M, odist = g.M * g.M * (g.M / 2 + 1);
+        cufftResult r = cufftPlanMany(&g.fwd, 3, n, nullptr, 1, idist, nullptr, 1, odist,
+                                      CUFFT_D2Z, g.count);
+        if (r == CUFFT_SUCCESS)
+            r = cufftPlanMany(&g.bwd, 3, n, nullptr, 1, odist, nullptr, 1, idist, CUFFT_Z2D,
+                              g.count);
+        if (r != CUFFT_SUCCESS) return fail(cufft_fail(r, "cufftPlanMany"));
+    }
+    if (b->staged_interp) {
+        const size_t smem = b->interp_smem;
+        auto set = [&](const void* fn) {
+            return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
+        };
+        cudaError_t a = cudaSuccess;
+        if (precision == SE_FP32) {
+            a = set((const void*)k_interp<float, 0>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<float, 8>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<float, 12>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<float, 16>);
+        } else {
+            a = set((const void*)k_interp<double, 0>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<double, 8>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<double, 12>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<double, 16>);
+            if (a == cudaSuccess) a = set((const void*)k_interp<double, 21>);
+        }
+        if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
+    }
+    *out = b;
+    return SE_OK;
+}
+
+#define LAUNCHED(b) ((b)->launches++)
+
+static int run_prepare_sort(se_batch b, const double* x, const double* q, cudaStream_t st)
+{
+    if (b->ntot > 0) {
+        k_prepare<<<ceil_div(b->ntot, 256), 256, 0, st>>>(b->sys, b->d_part_prefix, b->nsys,
+                                                          b->ntot, x, q, b->key, b->rec,
+                                                          b->gpk, b->err);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
+    }
+    SE_TRY(stable_sort(b->key, nullptr, b->ntot, std::max(b->nbins, 1), b->perm, nullptr,
+                       b->boff, b->sort_scratch, b->sort_bytes, st, &b->launches));
+    if (b->ntot > 0) {
+        k_gather<<<ceil_div(b->ntot, 256), 256, 0, st>>>(b->ntot, b->perm, b->rec, b->gpk,
+                                                         b->srec, b->sg);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
+    }
+    return SE_OK;
+}
+
+static int run_spread(se_batch b, double* grid, cudaStream_t st)
+{
+    if (b->precision == SE_FP32)
+        k_spread<float><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
+            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg, b->boff, grid);
+    else
+        k_spread<double><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
+            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg, b->boff, grid);
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
+static int run_kspace(se_batch b, double* grid, cudaStream_t st)
+{
+    for (auto& g : b->groups) {
+        SE_CUFFT(cufftSetStream(g.fwd, st));
+        SE_CUFFT(cufftExecD2Z(g.fwd, grid + g.grid_off,
+                              reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off)));
+    }
+    dim3 gs(std::min<long long>(1024, ceil_div(b->spec_elems / b->nsys + 1, 256)), b->nsys);
+    k_scale<<<gs, 256, 0, st>>>(b->sys, b->spec);
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    for (auto& g : b->groups) {
+        SE_CUFFT(cufftSetStream(g.bwd, st));
+        SE_CUFFT(cufftExecZ2D(g.bwd,
+                              reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off),
+                              grid + g.grid_off));
+    }
+    return SE_OK;
+}
+
+template <typename T>
+static int launch_interp_staged(se_batch b, const double* grid, double* out, double* phi,
+                                cudaStream_t st)
+{
+    const size_t smem = b->interp_smem;
+    const int P = b->max_P;
+    bool uniform = true;
+    for (auto& s : b->host_sys) uniform = uniform && s.P == P;
+    const dim3 grd(std::max(b->nbins, 1)), blk(INTERP_WARPS * 32);
+#define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, b->boff, grid, out, phi
+    if (uniform && P == 8) k_interp<T, 8><<<grd, blk, smem, st>>>(SE_IARGS);
+    else if (uniform && P == 12) k_interp<T, 12><<<grd, blk, smem, st>>>(SE_IARGS);
+    else if (uniform && P == 16) k_interp<T, 16><<<grd, blk, smem, st>>>(SE_IARGS);
+    else if (uniform && P == 21 && sizeof(T) == 8) k_interp<double, 21><<<grd, blk, smem, st>>>(SE_IARGS);
+    else k_interp<T, 0><<<grd, blk, smem, st>>>(SE_IARGS);
+#undef SE_IARGS
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
+static int run_interp(se_batch b, const double* grid, double* out, double* phi, cudaStream_t st)
+{
+    if (b->ntot == 0) return SE_OK;
+    if (b->staged_interp) {
+        if (b->precision == SE_FP32) return launch_interp_staged<float>(b, grid, out, phi, st);
+        return launch_interp_staged<double>(b, grid, out, phi, st);
+    }
+    k_interp_global<<<ceil_div(b->ntot, INTERP_WARPS), INTERP_WARPS * 32, 0, st>>>(
+        b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->sg, b->perm, grid, out, phi);
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
+static int batch_solve(se_batch b, const double* x, const double* q, double* out, double* phi,
+                       cudaStream_t st)
+{
+    b->launches = 0;
+    auto mark = [&](int i) -> int {
+        if (b->timing) SE_CUDA(cudaEventRecord(b->ev[i], st));
+        return SE_OK;
+    };
+    SE_CUDA(cudaMemsetAsync(b->err, 0, sizeof(int), st));
+    SE_TRY(mark(0));
+    SE_TRY(run_prepare_sort(b, x, q, st));
+    SE_TRY(mark(1));
+    SE_TRY(run_spread(b, b->grid, st));
+    SE_TRY(mark(2));
+    SE_TRY(run_kspace(b, b->grid, st));
+    SE_TRY(mark(3));
+    SE_TRY(run_interp(b, b->grid, out, phi, st));
+    SE_TRY(mark(4));
+    return SE_OK;
+}
+
+static int set_timing(se_batch b, int on)
+{
+    if (on && !b->ev[0])
+        for (auto& e : b->ev) SE_CUDA(cudaEventCreate(&e));
+    b->timing = on != 0;
+    return SE_OK;
+}
+
+static int stage_ms(se_batch b, float* ms)
+{
+    if (!b->timing || !ms) return SE_ERR_INVALID;
+    SE_CUDA(cudaEventSynchronize(b->ev[4]));
+    for (int i = 0; i < 4; i++) SE_CUDA(cudaEventElapsedTime(ms + i, b->ev[i], b->ev[i + 1]));
+    return SE_OK;
+}
+
+// FP32 FMA throughput of this GPU: independent FMA chains in every thread of
+// a grid that fills all SMs; the result is stored so nothing is elided.
+__global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters, float seed)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = seed + threadIdx.x * 1e-7f + k;
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = fmaf(a[k], m, c);
+    }
+    float s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace se
+
+// ============================================================ C ABI =====
+
+struct se_plan_s {
+    se_config cfg;
+    se_batch b = nullptr;
+    int N = -1;
+    double* h_x = nullptr;   // pinned staging for se_solve_host
+    double* h_q = nullptr;
+    double* h_out = nullptr;
+    double* d_x = nullptr;
+    double* d_q = nullptr;
+    double* d_out = nullptr;
+};
+
+using namespace se;
+
+extern "C" int se_config_derive(const se_config* cfg, double* h, double* w, double* eta,
+                                double* c, double* d)
+{
+    if (!cfg || cfg->M < 1 || cfg->P < 1 || cfg->L <= 0 || cfg->m <= 0) return SE_ERR_INVALID;
+    derive(cfg->M, cfg->P, cfg->L, cfg->xi, cfg->m, h, w, eta, c, d);
+    return SE_OK;
+}
+
+static se_system sys_of(const se_config* c, int N)
+{
+    se_system s;
+    s.N = N;
+    s.M = c->M;
+    s.P = c->P;
+    s.L = c->L;
+    s.xi = c->xi;
+    s.m = c->m;
+    s.mode = c->mode;
+    return s;
+}
+
+extern "C" size_t se_plan_device_bytes(const se_config* cfg)
+{
+    if (!cfg) return 0;
+    se_system s = sys_of(cfg, cfg->max_particles);
+    return batch_bytes(&s, 1, cfg->precision, nullptr, nullptr) +
+           (size_t)cfg->max_particles * 8 * 7;
+}
+
+extern "C" int se_plan_create(se_plan* plan, const se_config* cfg)
+{
+    if (!plan || !cfg || cfg->max_particles < 0) return SE_ERR_INVALID;
+    se_system s = sys_of(cfg, cfg->max_particles);
+    if (!valid_system(s)) return SE_ERR_INVALID;
+    se_plan p = new se_plan_s();
+    p->cfg = *cfg;
+    int r = batch_create(&p->b, &s, 1, cfg->precision);
+    if (r != SE_OK) {
+        delete p;
+        return r;
+    }
+    p->N = cfg->max_particles;
+    *plan = p;
+    return SE_OK;
+}
+
+extern "C" int se_plan_destroy(se_plan p)
+{
+    if (!p) return SE_OK;
+    batch_free(p->b);
+    if (p->h_x) cudaFreeHost(p->h_x);
+    if (p->h_q) cudaFreeHost(p->h_q);
+    if (p->h_out) cudaFreeHost(p->h_out);
+    if (p->d_x) cudaFree(p->d_x);
+    if (p->d_q) cudaFree(p->d_q);
+    if (p->d_out) cudaFree(p->d_out);
+    delete p;
+    return SE_OK;
+}
+
+// Re-point the single-system table at N particles (only when N changes).
+static int plan_set_N(se_plan p, int N, cudaStream_t st)
+{
+    if (N < 0 || N > p->cfg.max_particles) return SE_ERR_INVALID;
+    if (N == p->N) return SE_OK;
+    se_batch b = p->b;
+    SE_CUDA(cudaStreamSynchronize(st));
+    b->host_sys[0].N = N;
+    b->part_prefix[1] = N;
+    b->ntot = N;
+    SE_CUDA(cudaMemcpy(b->sys, b->host_sys.data(), sizeof(SysDev), cudaMemcpyHostToDevice));
+    SE_CUDA(cudaMemcpy(b->d_part_prefix, b->part_prefix.data(), sizeof(int) * 2,
+                       cudaMemcpyHostToDevice));
+    p->N = N;
+    return SE_OK;
+}
+
+extern "C" int se_solve(se_plan p, int N, const double* x, const double* q, double* out,
+                        double* phi_out, void* stream)
+{
+    if (!p || (N > 0 && (!x || !q || !out))) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    SE_TRY(plan_set_N(p, N, st));
+    return batch_solve(p->b, x, q, out, phi_out, st);
+}
+
+extern "C" int se_solve_host(se_plan p, int N, const double* xh, const double* qh,
+                             double* outh, void* stream)
+{
+    if (!p || (N > 0 && (!xh || !qh || !outh))) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    const int cap = p->cfg.max_particles;
+    const int outw = p->cfg.mode == SE_FORCE ? 3 : 1;
+    if (!p->d_x) {
+        SE_CUDA(cudaMalloc(&p->d_x, sizeof(double) * 3 * std::max(cap, 1)));
+        SE_CUDA(cudaMalloc(&p->d_q, sizeof(double) * std::max(cap, 1)));
+        SE_CUDA(cudaMalloc(&p->d_out, sizeof(double) * outw * std::max(cap, 1)));
+    }
+    SE_CUDA(cudaMemcpyAsync(p->d_x, xh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    SE_CUDA(cudaMemcpyAsync(p->d_q, qh, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    SE_TRY(plan_set_N(p, N, st));
+    SE_TRY(batch_solve(p->b, p->d_x, p->d_q, p->d_out, nullptr, st));
+    SE_CUDA(cudaMemcpyAsync(outh, p->d_out, sizeof(double) * outw * N, cudaMemcpyDeviceToHost, st));
+    SE_CUDA(cudaStreamSynchronize(st));
+    int err = 0;
+    SE_CUDA(cudaMemcpy(&err, p->b->err, sizeof(int), cudaMemcpyDeviceToHost));
+    return err ? SE_ERR_INPUT : SE_OK;
+}
+
+extern "C" int se_spread(se_plan p, int N, const double* x, const double* q, double* grid,
+                         void* stream)
+{
+    if (!p || !grid || (N > 0 && (!x || !q))) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    SE_TRY(plan_set_N(p, N, st));
+    p->b->launches = 0;
+    SE_TRY(run_prepare_sort(p->b, x, q, st));
+    return run_spread(p->b, grid, st);
+}
+
+extern "C" int se_kspace(se_plan p, double* grid, void* stream)
+{
+    if (!p || !grid) return SE_ERR_INVALID;
+    return run_kspace(p->b, grid, as_stream(stream));
+}
+
+extern "C" int se_interp(se_plan p, int N, const double* x, const double* q, const double* grid,
+                         double* out, double* phi_out, void* stream)
+{
+    if (!p || !grid || (N > 0 && (!x || !q || !out))) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    SE_TRY(plan_set_N(p, N, st));
+    p->b->launches = 0;
+    SE_TRY(run_prepare_sort(p->b, x, q, st));
+    return run_interp(p->b, grid, out, phi_out, st);
+}
+
+extern "C" int se_energy(const double* phi, const double* q, int N, double* e, void* stream)
+{
+    if (!phi || !q || !e || N < 0) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    static double* partial = nullptr;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!partial) SE_CUDA(cudaMalloc(&partial, sizeof(double) * 256));
+    const int nb = std::min(256, std::max(1, (int)ceil_div(N, 256)));
+    k_energy_partial<<<nb, 256, 0, st>>>(phi, q, N, partial);
+    SE_CUDA(cudaGetLastError());
+    k_energy_final<<<1, 256, 0, st>>>(partial, nb, e);
+    SE_CUDA(cudaGetLastError());
+    return SE_OK;
+}
+
+extern "C" int se_plan_launch_count(se_plan p) { return p ? p->b->launches : 0; }
+
+extern "C" size_t se_batch_device_bytes(const se_system* systems, int nsys, int precision)
+{
+    if (!systems || nsys < 1) return 0;
+    return batch_bytes(systems, nsys, precision, nullptr, nullptr);
+}
+
+extern "C" int se_batch_create(se_batch* b, const se_system* systems, int nsys, int precision)
+{
+    return batch_create(b, systems, nsys, precision);
+}
+
+extern "C" int se_batch_destroy(se_batch b) { return batch_free(b); }
+
+extern "C" int se_batch_solve(se_batch b, const double* x, const double* q, double* out,
+                              void* stream)
+{
+    if (!b || (b->ntot > 0 && (!x || !q || !out))) return SE_ERR_INVALID;
+    return batch_solve(b, x, q, out, nullptr, as_stream(stream));
+}
+
+extern "C" int se_batch_launch_count(se_batch b) { return b ? b->launches : 0; }
+
+extern "C" int se_plan_set_timing(se_plan p, int on)
+{
+    return p ? set_timing(p->b, on) : SE_ERR_INVALID;
+}
+
+extern "C" int se_plan_stage_ms(se_plan p, float* ms)
+{
+    return p ? stage_ms(p->b, ms) : SE_ERR_INVALID;
+}
+
+extern "C" int se_batch_set_timing(se_batch b, int on)
+{
+    return b ? set_timing(b, on) : SE_ERR_INVALID;
+}
+
+extern "C" int se_batch_stage_ms(se_batch b, float* ms) { return b ? stage_ms(b, ms) : SE_ERR_INVALID; }
+
+extern "C" int se_probe_fma_tflops(double* tflops, void* stream)
+{
+    if (!tflops) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    int dev = 0, sms = 0;
+    SE_CUDA(cudaGetDevice(&dev));
+    SE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    float* out = nullptr;
+    SE_CUDA(cudaMalloc(&out, sizeof(float) * blocks * threads));
+    cudaEvent_t e0, e1;
+    SE_CUDA(cudaEventCreate(&e0));
+    SE_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int r = 0; r < 5; r++) {
+        SE_CUDA(cudaEventRecord(e0, st));
+        k_fma_probe<<<blocks, threads, 0, st>>>(out, iters, 1.0f + r);
+        SE_CUDA(cudaGetLastError());
+        SE_CUDA(cudaEventRecord(e1, st));
+        SE_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        SE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (r > 0 && ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return SE_OK;
+}
+
+extern "C" const char* se_gpu_error_detail(void) { return se::g_err_msg; }
