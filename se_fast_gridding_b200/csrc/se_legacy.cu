@@ -130,23 +130,8 @@ public:
         ents_.push_back(e);
         return e.d;
     }
-    int copy_in()
-    {
-        if (err_) return err_;
-        for (auto& e : ents_)
-            if (e.host && e.in) SE_CUDA(cudaMemcpy(e.d, e.h, e.bytes, cudaMemcpyHostToDevice));
-        return SE_OK;
-    }
-    int finish()
-    {
-        if (err_) return err_;
-        SE_CUDA(cudaGetLastError());
-        SE_CUDA(cudaDeviceSynchronize());
-        for (auto& e : ents_)
-            if (e.host && e.out)
-                SE_CUDA(cudaMemcpy(const_cast<void*>(e.h), e.d, e.bytes, cudaMemcpyDeviceToHost));
-        return SE_OK;
-    }
+    int copy_in();
+    int finish();
     int error() const { return err_; }
 
 private:
@@ -203,6 +188,42 @@ struct ParamsDev {
     int dims[3], npdims[3];
     double c, d, h, a;
 };
+
+// Set by a kernel that skipped a particle whose stencil leaves the padded
+// grid (positions outside [0, L] give such indices; the reference writes out
+// of bounds there).  Reset and read by every legacy call.
+__device__ int g_legacy_err;
+
+__device__ __forceinline__ bool stencil_in_bounds(long long base, const ParamsDev& p)
+{
+    const long long n = (long long)p.npdims[0] * p.npdims[1] * p.npdims[2];
+    const long long last =
+        base + ((long long)(p.P - 1) * p.npdims[1] + (p.P - 1)) * p.npdims[2] + (p.P - 1);
+    return base >= 0 && last < n;
+}
+
+int Stager::copy_in()
+{
+    if (err_) return err_;
+    const int zero = 0;
+    SE_CUDA(cudaMemcpyToSymbol(g_legacy_err, &zero, sizeof(int)));
+    for (auto& e : ents_)
+        if (e.host && e.in) SE_CUDA(cudaMemcpy(e.d, e.h, e.bytes, cudaMemcpyHostToDevice));
+    return SE_OK;
+}
+
+int Stager::finish()
+{
+    if (err_) return err_;
+    SE_CUDA(cudaGetLastError());
+    SE_CUDA(cudaDeviceSynchronize());
+    for (auto& e : ents_)
+        if (e.host && e.out)
+            SE_CUDA(cudaMemcpy(const_cast<void*>(e.h), e.d, e.bytes, cudaMemcpyDeviceToHost));
+    int flag = 0;
+    SE_CUDA(cudaMemcpyFromSymbol(&flag, g_legacy_err, sizeof(int)));
+    return flag ? SE_ERR_INPUT : SE_OK;
+}
 
 static ParamsDev to_dev(const SE_FGG_params* p)
 {
@@ -299,6 +320,10 @@ __global__ void k_grid_split(double* H, const double* __restrict__ q,
     const long long o = (long long)n * P;
     const double qn = q[n];
     const long long base = idx[n];
+    if (!stencil_in_bounds(base, p)) {
+        if (threadIdx.x == 0) atomicOr(&g_legacy_err, 1);
+        return;
+    }
     const int n1 = p.npdims[1], n2 = p.npdims[2];
     for (int s = threadIdx.x; s < P * P * P; s += blockDim.x) {
         const int i = s / (P * P), j = (s / P) % P, k = s % P;
@@ -328,6 +353,10 @@ __global__ void k_grid_vanilla(double* H, const double* __restrict__ x,
         c0 = expand_one(xn, q[n], p, periodicity, z[0], z[1], z[2], nullptr, nullptr, nullptr);
     }
     __syncthreads();
+    if (!stencil_in_bounds(c0, p)) {
+        if (threadIdx.x == 0) atomicOr(&g_legacy_err, 1);
+        return;
+    }
     const int n1 = p.npdims[1], n2 = p.npdims[2];
     for (int s = threadIdx.x; s < P * P * P; s += blockDim.x) {
         const int i = s / (P * P), j = (s / P) % P, k = s % P;
@@ -395,6 +424,10 @@ __global__ void k_int_split(double* phi, const double* __restrict__ H,
     const int P = p.P, n1 = p.npdims[1], n2 = p.npdims[2];
     const long long o = (long long)m * P;
     const long long base = idx[m];
+    if (!stencil_in_bounds(base, p)) {
+        if (lane == 0) atomicOr(&g_legacy_err, 1);
+        return;
+    }
     double acc = 0;
     for (int s = lane; s < P * P * P; s += 32) {
         const int i = s / (P * P), j = (s / P) % P, k = s % P;
@@ -423,6 +456,10 @@ __global__ void k_int_vanilla(double* phi, const double* __restrict__ H,
     __syncwarp();
     const int P = p.P, n1 = p.npdims[1], n2 = p.npdims[2];
     const long long base = c0s[w];
+    if (!stencil_in_bounds(base, p)) {
+        if (lane == 0) atomicOr(&g_legacy_err, 1);
+        return;
+    }
     double acc = 0;
     for (int s = lane; s < P * P * P; s += 32) {
         const int i = s / (P * P), j = (s / P) % P, k = s % P;
@@ -448,6 +485,10 @@ __global__ void k_int_split_force(double* force, const double* __restrict__ q,
     const int P = p.P, n1 = p.npdims[1], n2 = p.npdims[2];
     const long long o = (long long)m * P;
     const long long base = idx[m];
+    if (!stencil_in_bounds(base, p)) {
+        if (lane == 0) atomicOr(&g_legacy_err, 1);
+        return;
+    }
     const double qm = q[m];
     double f0 = 0, f1 = 0, f2 = 0;
     for (int s = lane; s < P * P * P; s += 32) {
@@ -486,6 +527,10 @@ __global__ void k_int_force_vanilla(double* force, const double* __restrict__ H,
     __syncwarp();
     const int P = p.P, n1 = p.npdims[1], n2 = p.npdims[2];
     const long long base = c0s[w];
+    if (!stencil_in_bounds(base, p)) {
+        if (lane == 0) atomicOr(&g_legacy_err, 1);
+        return;
+    }
     double f0 = 0, f1 = 0, f2 = 0;
     for (int s = lane; s < P * P * P; s += 32) {
         const int i = s / (P * P), j = (s / P) % P, k = s % P;

@@ -157,40 +157,32 @@ __global__ void k_gather(int ntot, const int* __restrict__ perm, const double4* 
 
 // ------------------------------------------------------- factor rows -----
 
-// Gaussian factors exp(-c (t0 - (lo+i) h)^2) for the T cells o..o+T-1 of one
-// axis, i = (cell - g) mod M, zero where i >= P or the cell is outside [0, M).
-// Runs of consecutive i use the FGG recurrence (two exps per run).  Returns a
-// bitmask of the nonzero entries.
-template <int T, typename Acc>
-__device__ __forceinline__ unsigned factor_row(Acc* out, int o, int g, double t0, double scale,
-                                               const SysDev& S)
+// Each particle's separable Gaussian factors, once per solve, in bin order:
+// fac[(s*3 + a)*PS + i] = exp(-c (t0_a - (lo+i) h)^2), i < P, built with the
+// FGG recurrence in FP64 (SE_fgg.c:575-609 restated for the full Gaussian):
+// v_0 = exp(-c u_0^2), r_0 = exp(2 c h u_0 - c h^2), v_{i+1} = v_i r_i,
+// r_{i+1} = r_i exp(-2 c h^2), u_0 = t0 - lo h.  Stored in the working
+// precision T; PS is the batch's largest P.
+template <typename T>
+__global__ void k_factors(const SysDev* __restrict__ sys, const int* __restrict__ part_prefix,
+                          int nsys, int ntot, const double4* __restrict__ srec,
+                          const int* __restrict__ sperm, T* __restrict__ fac, int PS)
 {
-    unsigned mask = 0;
-    int i = pmod(o - g, S.M);
-    double v = 0.0, r = 0.0;
-    int prev = -2;
-#pragma unroll
-    for (int xo = 0; xo < T; xo++) {
-        double val = 0.0;
-        if (o + xo < S.M && i < S.P) {
-            if (i == prev + 1) {
-                v *= r;
-                r *= S.rho;
-            } else {
-                const double u = t0 - (S.lo + i) * S.h;
-                v = exp(-S.c * u * u);
-                r = exp(2.0 * S.c * S.h * u - S.c * S.h * S.h);
-            }
-            prev = i;
-            val = v * scale;
-            mask |= 1u << xo;
-        } else {
-            prev = -2;
-        }
-        out[xo] = (Acc)val;
-        if (++i == S.M) i = 0;
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= 3 * ntot) return;
+    const int s = u / 3, a = u - 3 * (u / 3);
+    const SysDev& S = sys[find_sys(part_prefix, nsys, sperm[s])];
+    const double4 rc = srec[s];
+    const double t0 = a == 0 ? rc.x : (a == 1 ? rc.y : rc.z);
+    const double u0 = t0 - S.lo * S.h;
+    double v = exp(-S.c * u0 * u0);
+    double r = exp(2.0 * S.c * S.h * u0 - S.c * S.h * S.h);
+    T* f = fac + ((long long)s * 3 + a) * PS;
+    for (int i = 0; i < S.P; i++) {
+        f[i] = (T)v;
+        v *= r;
+        r *= S.rho;
     }
-    return mask;
 }
 
 // ---------------------------------------------------------------- spread --
@@ -230,21 +222,47 @@ struct SpreadSmem {
     unsigned ymask[CHUNK];
 };
 
+// Factor-row entry for tile cell o + xo of one axis: the sum of the particle's
+// factors over every stencil index i < P that folds onto the cell
+// (i = cell - g mod M; more than one only when P > M).
+template <typename Acc>
+__device__ __forceinline__ Acc pad_entry(const Acc* __restrict__ f, int o, int xo, int g,
+                                         const SysDev& S)
+{
+    if (o + xo >= S.M) return Acc(0);
+    Acc v = Acc(0);
+    for (int i = pmod(o + xo - g, S.M); i < S.P; i += S.M) v += f[i];
+    return v;
+}
+
 template <typename Acc>
 __device__ __forceinline__ void spread_chunk(const SysDev& S, SpreadSmem<Acc>& sm,
                                              const double4* __restrict__ srec,
-                                             const int* __restrict__ sg, int c0, int n, int x0,
-                                             int y0, int z0, Acc (&acc)[4][4], int xh, int z4,
-                                             int yy)
+                                             const int* __restrict__ sg,
+                                             const Acc* __restrict__ fac, int PS, int c0, int n,
+                                             int x0, int y0, int z0, Acc (&acc)[4][4], int xh,
+                                             int z4, int yy)
 {
+    constexpr int ROW = TX + TY + TZ;
     __syncthreads();   // the previous chunk's rows are consumed
-    for (int u = threadIdx.x; u < n * 3; u += SPREAD_THREADS) {
-        const int p = u / 3, a = u - 3 * (u / 3);
-        const double4 rc = srec[c0 + p];
+    for (int u = threadIdx.x; u < n * ROW; u += SPREAD_THREADS) {
+        const int p = u / ROW, e = u - ROW * (u / ROW);
         const int pk = sg[c0 + p];
-        if (a == 0) factor_row<TX, Acc>(sm.px[p], x0, g_of(pk, 0), rc.x, rc.w, S);
-        else if (a == 1) sm.ymask[p] = factor_row<TY, Acc>(sm.py[p], y0, g_of(pk, 1), rc.y, 1.0, S);
-        else factor_row<TZ, Acc>(sm.pz[p], z0, g_of(pk, 2), rc.z, 1.0, S);
+        const Acc* f = fac + (long long)(c0 + p) * 3 * PS;
+        if (e < TX) {
+            sm.px[p][e] = pad_entry(f, x0, e, g_of(pk, 0), S) * (Acc)srec[c0 + p].w;
+        } else if (e < TX + TY) {
+            sm.py[p][e - TX] = pad_entry(f + PS, y0, e - TX, g_of(pk, 1), S);
+        } else {
+            sm.pz[p][e - TX - TY] = pad_entry(f + 2 * PS, z0, e - TX - TY, g_of(pk, 2), S);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < n) {
+        unsigned m = 0;
+#pragma unroll
+        for (int k = 0; k < TY; k++) m |= (sm.py[threadIdx.x][k] != Acc(0)) ? (1u << k) : 0u;
+        sm.ymask[threadIdx.x] = m;
     }
     __syncthreads();
     const int wrow = yy & ~3;   // the 4 rows of this warp
@@ -272,7 +290,7 @@ template <typename Acc>
 __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
-    const int* __restrict__ boff, double* __restrict__ grid)
+    const Acc* __restrict__ fac, int PS, const int* __restrict__ boff, double* __restrict__ grid)
 {
     __shared__ __align__(16) SpreadSmem<Acc> sm;
     const int tile = blockIdx.x;
@@ -308,8 +326,9 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
                         const int kb = S.bin_base + (bx * S.nf[1] + by) * S.nf[2];
                         const int beg = boff[kb + bz0], end = boff[kb + bz1 + 1];
                         for (int c0 = beg; c0 < end; c0 += CHUNK) {
-                            spread_chunk<Acc>(S, sm, srec, sg, c0, min(CHUNK, end - c0), x0,
-                                              y0, z0, acc, xh, z4, yy);
+                            spread_chunk<Acc>(S, sm, srec, sg, fac, PS, c0,
+                                              min(CHUNK, end - c0), x0, y0, z0, acc, xh, z4,
+                                              yy);
                             if (sizeof(Acc) == 4) {   // compensated: fold the chunk sum
 #pragma unroll
                                 for (int j = 0; j < 4; j++)
@@ -393,8 +412,9 @@ template <typename T, int PT>
 __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
     const SysDev* __restrict__ sys, const int* __restrict__ bin_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
-    const int* __restrict__ sperm, const int* __restrict__ boff,
-    const double* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out)
+    const int* __restrict__ sperm, const T* __restrict__ fac, int PS,
+    const int* __restrict__ boff, const double* __restrict__ grid, double* __restrict__ out,
+    double* __restrict__ phi_out)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ InterpWarpSmem wsm[INTERP_WARPS];
@@ -427,10 +447,11 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
         const int r0 = g_of(pk, 0) - o[0], r1 = g_of(pk, 1) - o[1], r2 = g_of(pk, 2) - o[2];
         if (lane < P) {
             const double t0[3] = {rc.x, rc.y, rc.z};
+            const T* f = fac + (long long)p * 3 * PS;
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 const double u = t0[a] - (S.lo + lane) * S.h;
-                const double v = exp(-S.c * u * u);
+                const double v = (double)f[a * PS + lane];
                 W.w[a][lane] = v;
                 W.wf[a][lane] = v * (-S.c * u);
             }
@@ -496,11 +517,12 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
 
 // Interpolation without staging, for windows that exceed shared memory
 // (large P in FP64): the same sums read from the periodic grid in L2.
+template <typename T>
 __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp_global(
     const SysDev* __restrict__ sys, const int* __restrict__ part_prefix, int nsys, int ntot,
     const double4* __restrict__ srec, const int* __restrict__ sg,
-    const int* __restrict__ sperm, const double* __restrict__ grid, double* __restrict__ out,
-    double* __restrict__ phi_out)
+    const int* __restrict__ sperm, const T* __restrict__ fac, int PS,
+    const double* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out)
 {
     __shared__ InterpWarpSmem wsm[INTERP_WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -516,9 +538,10 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp_global(
     const int g0 = g_of(pk, 0), g1 = g_of(pk, 1), g2 = g_of(pk, 2);
     if (lane < P) {
         const double t0[3] = {rc.x, rc.y, rc.z};
+        const T* f = fac + (long long)p * 3 * PS;
         for (int a = 0; a < 3; a++) {
             const double u = t0[a] - (S.lo + lane) * S.h;
-            const double v = exp(-S.c * u * u);
+            const double v = (double)f[a * PS + lane];
             W.w[a][lane] = v;
             W.wf[a][lane] = v * (-S.c * u);
         }
@@ -635,6 +658,8 @@ struct se_batch_s {
     double4* srec = nullptr;
     int* sg = nullptr;
     int* boff = nullptr;
+    void* fac = nullptr;      // per-particle factors [ntot][3][PS], working precision
+    int PS = 0;
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     double* grid = nullptr;
@@ -670,7 +695,7 @@ static void derive(int M, int P, double L, double xi, double m, double* h, doubl
 
 static bool valid_system(const se_system& s)
 {
-    return s.N >= 0 && s.M >= 2 && s.M <= 1024 && s.P >= 1 && s.P <= MAX_P && s.P <= s.M &&
+    return s.N >= 0 && s.M >= 2 && s.M <= 1024 && s.P >= 1 && s.P <= MAX_P &&
            s.L > 0 && s.xi > 0 && s.m > 0 && (s.mode == SE_POTENTIAL || s.mode == SE_FORCE);
 }
 
@@ -697,6 +722,9 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     if (ntiles_out) *ntiles_out = (int)ntiles;
     size_t b = 0;
     b += (size_t)ntot * (4 + 32 + 4 + 4 + 32 + 4);
+    int maxP = 1;
+    for (int i = 0; i < nsys; i++) maxP = std::max(maxP, sys[i].P);
+    b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
     b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
     b += (size_t)(nbins + 1) * 4;
     b += (size_t)grid * 8 + (size_t)spec * 16;
@@ -717,7 +745,7 @@ static int batch_free(se_batch b)
         if (e) cudaEventDestroy(e);
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
-                    b->grid, b->spec, b->energy_partial, b->err};
+                    b->grid, b->spec, b->energy_partial, b->err, b->fac};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -834,6 +862,8 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     SE_ALLOC(b->srec, sizeof(double4) * nt);
     SE_ALLOC(b->sg, sizeof(int) * nt);
     SE_ALLOC(b->boff, sizeof(int) * (b->nbins + 1));
+    b->PS = b->max_P;
+    SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
     b->sort_bytes = sort_scratch_bytes(b->ntot, std::max(b->nbins, 1));
     SE_ALLOC(b->sort_scratch, b->sort_bytes);
     SE_ALLOC(b->grid, sizeof(double) * b->grid_elems);
@@ -891,6 +921,8 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
 
 #define LAUNCHED(b) ((b)->launches++)
 
+static int run_factors(se_batch b, cudaStream_t st);
+
 static int run_prepare_sort(se_batch b, const double* x, const double* q, cudaStream_t st)
 {
     if (b->ntot > 0) {
@@ -908,17 +940,19 @@ static int run_prepare_sort(se_batch b, const double* x, const double* q, cudaSt
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
     }
-    return SE_OK;
+    return run_factors(b, st);
 }
 
 static int run_spread(se_batch b, double* grid, cudaStream_t st)
 {
     if (b->precision == SE_FP32)
         k_spread<float><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
-            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg, b->boff, grid);
+            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg, static_cast<const float*>(b->fac),
+            b->PS, b->boff, grid);
     else
         k_spread<double><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
-            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg, b->boff, grid);
+            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
+            static_cast<const double*>(b->fac), b->PS, b->boff, grid);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     return SE_OK;
@@ -953,13 +987,31 @@ static int launch_interp_staged(se_batch b, const double* grid, double* out, dou
     bool uniform = true;
     for (auto& s : b->host_sys) uniform = uniform && s.P == P;
     const dim3 grd(std::max(b->nbins, 1)), blk(INTERP_WARPS * 32);
-#define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, b->boff, grid, out, phi
+    const T* fac = static_cast<const T*>(b->fac);
+#define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, fac, b->PS, b->boff, \
+                 grid, out, phi
     if (uniform && P == 8) k_interp<T, 8><<<grd, blk, smem, st>>>(SE_IARGS);
     else if (uniform && P == 12) k_interp<T, 12><<<grd, blk, smem, st>>>(SE_IARGS);
     else if (uniform && P == 16) k_interp<T, 16><<<grd, blk, smem, st>>>(SE_IARGS);
-    else if (uniform && P == 21 && sizeof(T) == 8) k_interp<double, 21><<<grd, blk, smem, st>>>(SE_IARGS);
+    else if (sizeof(T) == 8 && uniform && P == 21) k_interp<T, 21><<<grd, blk, smem, st>>>(SE_IARGS);
     else k_interp<T, 0><<<grd, blk, smem, st>>>(SE_IARGS);
 #undef SE_IARGS
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
+static int run_factors(se_batch b, cudaStream_t st)
+{
+    if (b->ntot == 0) return SE_OK;
+    const unsigned nb = ceil_div(3L * b->ntot, 256);
+    if (b->precision == SE_FP32)
+        k_factors<float><<<nb, 256, 0, st>>>(b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec,
+                                             b->perm, static_cast<float*>(b->fac), b->PS);
+    else
+        k_factors<double><<<nb, 256, 0, st>>>(b->sys, b->d_part_prefix, b->nsys, b->ntot,
+                                              b->srec, b->perm, static_cast<double*>(b->fac),
+                                              b->PS);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     return SE_OK;
@@ -972,8 +1024,15 @@ static int run_interp(se_batch b, const double* grid, double* out, double* phi, 
         if (b->precision == SE_FP32) return launch_interp_staged<float>(b, grid, out, phi, st);
         return launch_interp_staged<double>(b, grid, out, phi, st);
     }
-    k_interp_global<<<ceil_div(b->ntot, INTERP_WARPS), INTERP_WARPS * 32, 0, st>>>(
-        b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->sg, b->perm, grid, out, phi);
+    const unsigned nb = ceil_div(b->ntot, INTERP_WARPS);
+    if (b->precision == SE_FP32)
+        k_interp_global<float><<<nb, INTERP_WARPS * 32, 0, st>>>(
+            b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->sg, b->perm,
+            static_cast<const float*>(b->fac), b->PS, grid, out, phi);
+    else
+        k_interp_global<double><<<nb, INTERP_WARPS * 32, 0, st>>>(
+            b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->sg, b->perm,
+            static_cast<const double*>(b->fac), b->PS, grid, out, phi);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     return SE_OK;

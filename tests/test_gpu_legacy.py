@@ -235,6 +235,26 @@ def test_fftw_shim(F, shape):
     np.testing.assert_allclose(out.reshape(shape), r * r.size, rtol=0, atol=1e-11 * r.size)
 
 
+def test_out_of_box_position_reported(F):
+    """A position outside [0, L] gives a stencil outside the padded grid (the
+    reference writes out of bounds there); the kernels skip it and the call
+    reports the error."""
+    import oracle as O
+    import se_fast_gridding_b200 as S
+    opt, p = F.fcn_params(16, 8, 1.0, 4.0, 0.95 * np.sqrt(O.PI * 8), 2)
+    x = np.array([0.5, 3.0, 0.5, 0.5, 0.5, 0.5])
+    q = np.array([1.0, -1.0])
+    w = F.Work(p, where="host")
+    st = F.state(x, q)
+    F.call("SE_FGG_base_gaussian", C.byref(w.s), C.byref(p))
+    F.call("SE_FGG_expand_all", C.byref(w.s), C.byref(st), C.byref(p))
+    with pytest.raises(S.SEError):
+        F.call("SE_FGG_grid_split", C.byref(w.s), C.byref(st), C.byref(p))
+    # the in-box particle was still spread, and the library keeps working
+    assert np.abs(w.get("H")).sum() > 0
+    F.call("SE_FGG_base_gaussian", C.byref(w.s), C.byref(p))
+
+
 def test_invalid_params_reported(F):
     """P beyond SE_P_MAX is refused with an error, not computed."""
     p = F.pack_params(4, 8, 8, 8, 40, 10.0, 0.125)
