@@ -1,0 +1,59 @@
+// se_device.cuh -- definitions shared by the device-resident kernels
+// (included inside namespace se by se_solve.cu).
+#pragma once
+
+constexpr int FB = 8;                     // fine bin edge, in stencil corners
+constexpr int TX = 16, TY = 16, TZ = 16;  // spread tile (output cells)
+constexpr int WY = 4, WZ = 8;             // one warp's lane block: 4 y x 8 z
+constexpr int SPREAD_WARPS = (TY / WY) * (TZ / WZ);
+constexpr int SPREAD_THREADS = SPREAD_WARPS * 32;
+constexpr int CHUNK = 64;                 // particles staged per spread round
+constexpr int MAX_SEG = 96;               // bin segments reaching one tile
+constexpr int INTERP_WARPS = 8;
+constexpr int MAX_P = 32;
+constexpr double PI_D = 3.14159265358979323846;
+
+// Per-system parameters and offsets of a batch (one entry per system).
+struct SysDev {
+    int N, M, P, lo, mode;
+    int part_off, out_off;
+    long long grid_off, spec_off;
+    int nf[3];        // fine bins per axis
+    int bin_base;     // first global fine-bin id
+    int nt[3];        // spread tiles per axis
+    int tile_base;    // first global spread-tile id
+    double h, c, d, h3;
+    double rho;       // exp(-2 c h^2)
+    double kfac;      // 2 pi / L
+    double scalar;    // -(1 - eta) / (4 xi^2)
+    double dnorm;     // 4 pi / M^3
+};
+
+// largest s with prefix[s] <= v
+__device__ __forceinline__ int find_sys(const int* __restrict__ prefix, int nsys, int v)
+{
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// periodic index in [0, n) for any int i (SE_fgg.c:17-25 vmod)
+__device__ __forceinline__ int pmod(int i, int n)
+{
+    const int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+// i in (-n, 2n) to [0, n) without a division
+__device__ __forceinline__ int wrap1(int i, int n)
+{
+    i = i < 0 ? i + n : i;
+    return i >= n ? i - n : i;
+}
+
+__device__ __forceinline__ int pack_g(int gx, int gy, int gz) { return gx | (gy << 10) | (gz << 20); }
+__device__ __forceinline__ int g_of(int pk, int a) { return (pk >> (10 * a)) & 1023; }

@@ -7,18 +7,12 @@
 //   k_prepare   per particle: stencil corner and offset as fgg_expansion_3p
 //               (SE_fgg.c:539-621), charge x d, fine-bin key
 //   stable_sort by fine-bin key (se_sort.cu), then k_gather into bin order
-//   k_spread    one CTA per output tile of the periodic grid: every particle
-//               whose stencil reaches the tile contributes through per-tile
-//               separable factor rows built with the FGG recurrence
-//               exp(-c u^2), r = exp(2chu - ch^2), r <- r exp(-2ch^2); cells
-//               accumulate in registers and are written once, so the periodic
-//               fold of SE_FGG_wrap_fcn (SE_fgg.c:327-352) needs no atomics
+//   k_factors   each particle's separable Gaussian factors, FGG recurrence
+//   k_spread    one CTA per output tile of the periodic grid, the fold fused
+//               (se_spread.cuh)
 //   cuFFT D2Z, k_scale (Z of scaling(), SE_general.c:145-175, applied to the
 //               half spectrum as product_rc does, SE_general.c:336-362), Z2D
-//   k_interp    one CTA per fine bin: the bin's (8+P-1)^3 window of the
-//               periodic grid is staged in shared memory (the unfold of
-//               SE_FGG_extend_fcn, SE_fgg.c:417-443), one warp per particle
-//               gathers sum H W (SE_fgg.c:968-1100)
+//   k_interp    one CTA per fine bin, the unfold fused (se_interp.cuh)
 //
 // Grid layout: M^3 FP64 row-major [x][y][z], the transpose of the reference's
 // column-major H_per; the FFT of the transpose is the transpose of the FFT and
@@ -61,51 +55,7 @@ static int cufft_fail(cufftResult r, const char* what)
         if (se_r_ != CUFFT_SUCCESS) return cufft_fail(se_r_, #call);          \
     } while (0)
 
-// ----------------------------------------------------------- geometry -----
-
-constexpr int FB = 8;                     // fine bin edge, in stencil corners
-constexpr int TX = 8, TY = 16, TZ = 16;   // spread tile (output cells)
-constexpr int SPREAD_THREADS = 128;
-constexpr int CHUNK = 64;                 // particles staged per spread round
-constexpr int INTERP_WARPS = 8;
-constexpr int MAX_P = 32;
-constexpr double PI_D = 3.14159265358979323846;
-
-struct SysDev {
-    int N, M, P, lo, mode;
-    int part_off, out_off;
-    long long grid_off, spec_off;
-    int nf[3];
-    int bin_base;
-    int nt[3];
-    int tile_base;
-    double h, c, d, h3;
-    double rho;      // exp(-2 c h^2)
-    double kfac;     // 2 pi / L
-    double scalar;   // -(1 - eta) / (4 xi^2)
-    double dnorm;    // 4 pi / M^3
-};
-
-__device__ __forceinline__ int find_sys(const int* __restrict__ prefix, int nsys, int v)
-{
-    // largest s with prefix[s] <= v
-    int lo = 0, hi = nsys - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(prefix + mid) <= v) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ int pmod(int i, int n)
-{
-    const int r = i % n;
-    return r < 0 ? r + n : r;
-}
-
-__device__ __forceinline__ int pack_g(int gx, int gy, int gz) { return gx | (gy << 10) | (gz << 20); }
-__device__ __forceinline__ int g_of(int pk, int a) { return (pk >> (10 * a)) & 1023; }
+#include "se_device.cuh"
 
 // --------------------------------------------------------------- prepare --
 
@@ -185,179 +135,7 @@ __global__ void k_factors(const SysDev* __restrict__ sys, const int* __restrict_
     }
 }
 
-// ---------------------------------------------------------------- spread --
-
-// Up to two fine-bin ranges whose corners reach the output cells [o, o+T).
-struct BinRanges {
-    int a0, a1, b0, b1;   // [a0,a1] and [b0,b1], b0 > b1 when absent
-};
-
-__device__ __forceinline__ BinRanges bins_reaching(int o, int T, int M, int P, int nf)
-{
-    BinRanges r;
-    const int Ta = min(T, M - o);
-    const int len = Ta + P - 1;   // corners g with (g + i) mod M in the tile, i < P
-    if (len >= M) {
-        r.a0 = 0; r.a1 = nf - 1; r.b0 = 1; r.b1 = 0;
-        return r;
-    }
-    const int start = pmod(o - P + 1, M);
-    const int end = start + len - 1;
-    if (end < M) {
-        r.a0 = start / FB; r.a1 = end / FB; r.b0 = 1; r.b1 = 0;
-    } else {
-        const int e2 = end - M;
-        r.a0 = start / FB; r.a1 = nf - 1;
-        r.b0 = 0; r.b1 = e2 / FB;
-        if (r.b1 >= r.a0) { r.a0 = 0; r.a1 = nf - 1; r.b0 = 1; r.b1 = 0; }
-    }
-    return r;
-}
-
-template <typename Acc>
-struct SpreadSmem {
-    Acc px[CHUNK][TX];
-    Acc py[CHUNK][TY];
-    Acc pz[CHUNK][TZ];
-    unsigned ymask[CHUNK];
-};
-
-// Factor-row entry for tile cell o + xo of one axis: the sum of the particle's
-// factors over every stencil index i < P that folds onto the cell
-// (i = cell - g mod M; more than one only when P > M).
-template <typename Acc>
-__device__ __forceinline__ Acc pad_entry(const Acc* __restrict__ f, int o, int xo, int g,
-                                         const SysDev& S)
-{
-    if (o + xo >= S.M) return Acc(0);
-    Acc v = Acc(0);
-    for (int i = pmod(o + xo - g, S.M); i < S.P; i += S.M) v += f[i];
-    return v;
-}
-
-template <typename Acc>
-__device__ __forceinline__ void spread_chunk(const SysDev& S, SpreadSmem<Acc>& sm,
-                                             const double4* __restrict__ srec,
-                                             const int* __restrict__ sg,
-                                             const Acc* __restrict__ fac, int PS, int c0, int n,
-                                             int x0, int y0, int z0, Acc (&acc)[4][4], int xh,
-                                             int z4, int yy)
-{
-    constexpr int ROW = TX + TY + TZ;
-    __syncthreads();   // the previous chunk's rows are consumed
-    for (int u = threadIdx.x; u < n * ROW; u += SPREAD_THREADS) {
-        const int p = u / ROW, e = u - ROW * (u / ROW);
-        const int pk = sg[c0 + p];
-        const Acc* f = fac + (long long)(c0 + p) * 3 * PS;
-        if (e < TX) {
-            sm.px[p][e] = pad_entry(f, x0, e, g_of(pk, 0), S) * (Acc)srec[c0 + p].w;
-        } else if (e < TX + TY) {
-            sm.py[p][e - TX] = pad_entry(f + PS, y0, e - TX, g_of(pk, 1), S);
-        } else {
-            sm.pz[p][e - TX - TY] = pad_entry(f + 2 * PS, z0, e - TX - TY, g_of(pk, 2), S);
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < n) {
-        unsigned m = 0;
-#pragma unroll
-        for (int k = 0; k < TY; k++) m |= (sm.py[threadIdx.x][k] != Acc(0)) ? (1u << k) : 0u;
-        sm.ymask[threadIdx.x] = m;
-    }
-    __syncthreads();
-    const int wrow = yy & ~3;   // the 4 rows of this warp
-    for (int p = 0; p < n; p++) {
-        if (((sm.ymask[p] >> wrow) & 0xFu) == 0u) continue;   // warp-uniform
-        const Acc wy = sm.py[p][yy];
-        Acc wz[4], wx[4];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            wz[k] = sm.pz[p][4 * z4 + k];
-            wx[k] = sm.px[p][4 * xh + k];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const Acc cz = wy * wz[k];
-#pragma unroll
-            for (int j = 0; j < 4; j++) acc[j][k] = fma(wx[j], cz, acc[j][k]);
-        }
-    }
-}
-
-// One CTA per TX x TY x TZ tile of one system's periodic grid.  Thread t owns
-// the 4 x 4 cells (x0 + 4 xh + j, y0 + yy, z0 + 4 z4 + k).
-template <typename Acc>
-__global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
-    const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
-    const double4* __restrict__ srec, const int* __restrict__ sg,
-    const Acc* __restrict__ fac, int PS, const int* __restrict__ boff, double* __restrict__ grid)
-{
-    __shared__ __align__(16) SpreadSmem<Acc> sm;
-    const int tile = blockIdx.x;
-    const int s = find_sys(tile_prefix, nsys, tile);
-    const SysDev& S = sys[s];
-    const int lt = tile - S.tile_base;
-    const int ax = lt / (S.nt[1] * S.nt[2]);
-    const int ay = (lt / S.nt[2]) % S.nt[1];
-    const int az = lt % S.nt[2];
-    const int x0 = ax * TX, y0 = ay * TY, z0 = az * TZ;
-    const int t = threadIdx.x;
-    const int xh = t & 1, z4 = (t >> 1) & 3, yy = t >> 3;
-
-    Acc acc[4][4];
-    double accd[4][4];
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-        for (int k = 0; k < 4; k++) { acc[j][k] = Acc(0); accd[j][k] = 0.0; }
-
-    const BinRanges rx = bins_reaching(x0, TX, S.M, S.P, S.nf[0]);
-    const BinRanges ry = bins_reaching(y0, TY, S.M, S.P, S.nf[1]);
-    const BinRanges rz = bins_reaching(z0, TZ, S.M, S.P, S.nf[2]);
-    for (int ix = 0; ix < 2; ix++) {
-        const int bx0 = ix ? rx.b0 : rx.a0, bx1 = ix ? rx.b1 : rx.a1;
-        for (int bx = bx0; bx <= bx1; bx++)
-            for (int iy = 0; iy < 2; iy++) {
-                const int by0 = iy ? ry.b0 : ry.a0, by1 = iy ? ry.b1 : ry.a1;
-                for (int by = by0; by <= by1; by++)
-                    for (int iz = 0; iz < 2; iz++) {
-                        const int bz0 = iz ? rz.b0 : rz.a0, bz1 = iz ? rz.b1 : rz.a1;
-                        if (bz0 > bz1) continue;
-                        const int kb = S.bin_base + (bx * S.nf[1] + by) * S.nf[2];
-                        const int beg = boff[kb + bz0], end = boff[kb + bz1 + 1];
-                        for (int c0 = beg; c0 < end; c0 += CHUNK) {
-                            spread_chunk<Acc>(S, sm, srec, sg, fac, PS, c0,
-                                              min(CHUNK, end - c0), x0, y0, z0, acc, xh, z4,
-                                              yy);
-                            if (sizeof(Acc) == 4) {   // compensated: fold the chunk sum
-#pragma unroll
-                                for (int j = 0; j < 4; j++)
-#pragma unroll
-                                    for (int k = 0; k < 4; k++) {
-                                        accd[j][k] += (double)acc[j][k];
-                                        acc[j][k] = Acc(0);
-                                    }
-                            }
-                        }
-                    }
-            }
-    }
-    const int gy = y0 + yy;
-    if (gy >= S.M) return;
-    double* gs = grid + S.grid_off;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const int gx = x0 + 4 * xh + j;
-        if (gx >= S.M) continue;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int gz = z0 + 4 * z4 + k;
-            if (gz < S.M)
-                gs[((long long)gx * S.M + gy) * S.M + gz] =
-                    sizeof(Acc) == 4 ? accd[j][k] : (double)acc[j][k];
-        }
-    }
-}
+#include "se_spread.cuh"
 
 // --------------------------------------------------------------- k-space --
 
@@ -391,204 +169,7 @@ __global__ void k_scale(const SysDev* __restrict__ sys, double2* __restrict__ sp
     }
 }
 
-// ---------------------------------------------------------------- interp --
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-struct InterpWarpSmem {
-    double w[3][MAX_P];    // Gaussian factors per axis
-    double wf[3][MAX_P];   // times -c u (force)
-};
-
-// One CTA per fine bin; E = FB + P - 1 cells per axis staged (pitch E|1).
-// PT = P at compile time (0: runtime P).
-template <typename T, int PT>
-__global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
-    const SysDev* __restrict__ sys, const int* __restrict__ bin_prefix, int nsys,
-    const double4* __restrict__ srec, const int* __restrict__ sg,
-    const int* __restrict__ sperm, const T* __restrict__ fac, int PS,
-    const int* __restrict__ boff, const double* __restrict__ grid, double* __restrict__ out,
-    double* __restrict__ phi_out)
-{
-    extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ InterpWarpSmem wsm[INTERP_WARPS];
-    const int bin = blockIdx.x;
-    const int beg = boff[bin], end = boff[bin + 1];
-    if (beg == end) return;
-    const int s = find_sys(bin_prefix, nsys, bin);
-    const SysDev& S = sys[s];
-    const int P = PT ? PT : S.P;
-    const int M = S.M;
-    const int lb = bin - S.bin_base;
-    const int o[3] = {(lb / (S.nf[1] * S.nf[2])) * FB, ((lb / S.nf[2]) % S.nf[1]) * FB,
-                      (lb % S.nf[2]) * FB};
-    const int E = FB + P - 1, Ep = E | 1;
-    T* tile = reinterpret_cast<T*>(dsm);
-    const double* gs = grid + S.grid_off;
-    // stage the periodic window [o, o + E) mod M
-    for (int e = threadIdx.x; e < E * E * E; e += blockDim.x) {
-        const int c = e % E, b = (e / E) % E, a = e / (E * E);
-        const int gx = pmod(o[0] + a, M), gy = pmod(o[1] + b, M), gz = pmod(o[2] + c, M);
-        tile[(a * E + b) * Ep + c] = (T)gs[((long long)gx * M + gy) * M + gz];
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    InterpWarpSmem& W = wsm[warp];
-    const bool force = S.mode == SE_FORCE;
-    for (int p = beg + warp; p < end; p += INTERP_WARPS) {
-        const double4 rc = srec[p];
-        const int pk = sg[p];
-        const int r0 = g_of(pk, 0) - o[0], r1 = g_of(pk, 1) - o[1], r2 = g_of(pk, 2) - o[2];
-        if (lane < P) {
-            const double t0[3] = {rc.x, rc.y, rc.z};
-            const T* f = fac + (long long)p * 3 * PS;
-#pragma unroll
-            for (int a = 0; a < 3; a++) {
-                const double u = t0[a] - (S.lo + lane) * S.h;
-                const double v = (double)f[a * PS + lane];
-                W.w[a][lane] = v;
-                W.wf[a][lane] = v * (-S.c * u);
-            }
-        }
-        __syncwarp();
-        T wz[PT ? PT : MAX_P], wzf[PT ? PT : MAX_P];
-        if (PT) {
-#pragma unroll
-            for (int k = 0; k < (PT ? PT : 1); k++) {
-                wz[k] = (T)W.w[2][k];
-                wzf[k] = (T)W.wf[2][k];
-            }
-        }
-        double a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
-        for (int r = lane; r < P * P; r += 32) {
-            const int i = r / P, j = r - (r / P) * P;
-            const T* row = tile + ((r0 + i) * E + (r1 + j)) * Ep + r2;
-            T s0 = 0, s1 = 0;
-            if (PT) {
-#pragma unroll
-                for (int k = 0; k < (PT ? PT : 1); k++) {
-                    const T hv = row[k];
-                    s0 = fma(hv, wz[k], s0);
-                    if (force) s1 = fma(hv, wzf[k], s1);
-                }
-            } else {
-                for (int k = 0; k < P; k++) {
-                    const T hv = row[k];
-                    s0 = fma(hv, (T)W.w[2][k], s0);
-                    if (force) s1 = fma(hv, (T)W.wf[2][k], s1);
-                }
-            }
-            const double wxi = W.w[0][i], wyj = W.w[1][j];
-            a_pot = fma((double)s0, wxi * wyj, a_pot);
-            if (force) {
-                a_fx = fma((double)s0, W.wf[0][i] * wyj, a_fx);
-                a_fy = fma((double)s0, wxi * W.wf[1][j], a_fy);
-                a_fz = fma((double)s1, wxi * wyj, a_fz);
-            }
-        }
-        a_pot = warp_sum(a_pot);
-        if (force) {
-            a_fx = warp_sum(a_fx);
-            a_fy = warp_sum(a_fy);
-            a_fz = warp_sum(a_fz);
-        }
-        if (lane == 0) {
-            const int loc = sperm[p] - S.part_off;
-            const double scale = S.h3 * S.d;
-            if (force) {
-                const double qs = rc.w / S.d * scale;   // q h^3 d
-                out[S.out_off + loc] = qs * a_fx;
-                out[S.out_off + loc + S.N] = qs * a_fy;
-                out[S.out_off + loc + 2 * S.N] = qs * a_fz;
-                if (phi_out) phi_out[S.part_off + loc] = scale * a_pot;
-            } else {
-                out[S.out_off + loc] = scale * a_pot;
-            }
-        }
-        __syncwarp();
-    }
-}
-
-// Interpolation without staging, for windows that exceed shared memory
-// (large P in FP64): the same sums read from the periodic grid in L2.
-template <typename T>
-__global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp_global(
-    const SysDev* __restrict__ sys, const int* __restrict__ part_prefix, int nsys, int ntot,
-    const double4* __restrict__ srec, const int* __restrict__ sg,
-    const int* __restrict__ sperm, const T* __restrict__ fac, int PS,
-    const double* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out)
-{
-    __shared__ InterpWarpSmem wsm[INTERP_WARPS];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = blockIdx.x * INTERP_WARPS + warp;
-    if (p >= ntot) return;
-    const int orig = sperm[p];
-    const int s = find_sys(part_prefix, nsys, orig);
-    const SysDev& S = sys[s];
-    const int P = S.P, M = S.M;
-    InterpWarpSmem& W = wsm[warp];
-    const double4 rc = srec[p];
-    const int pk = sg[p];
-    const int g0 = g_of(pk, 0), g1 = g_of(pk, 1), g2 = g_of(pk, 2);
-    if (lane < P) {
-        const double t0[3] = {rc.x, rc.y, rc.z};
-        const T* f = fac + (long long)p * 3 * PS;
-        for (int a = 0; a < 3; a++) {
-            const double u = t0[a] - (S.lo + lane) * S.h;
-            const double v = (double)f[a * PS + lane];
-            W.w[a][lane] = v;
-            W.wf[a][lane] = v * (-S.c * u);
-        }
-    }
-    __syncwarp();
-    const bool force = S.mode == SE_FORCE;
-    const double* gs = grid + S.grid_off;
-    double a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
-    for (int r = lane; r < P * P; r += 32) {
-        const int i = r / P, j = r % P;
-        const double* row = gs + ((long long)pmod(g0 + i, M) * M + pmod(g1 + j, M)) * M;
-        double s0 = 0, s1 = 0;
-        int z = g2;
-        for (int k = 0; k < P; k++) {
-            const double hv = __ldg(row + z);
-            s0 = fma(hv, W.w[2][k], s0);
-            if (force) s1 = fma(hv, W.wf[2][k], s1);
-            if (++z == M) z = 0;
-        }
-        const double wxi = W.w[0][i], wyj = W.w[1][j];
-        a_pot = fma(s0, wxi * wyj, a_pot);
-        if (force) {
-            a_fx = fma(s0, W.wf[0][i] * wyj, a_fx);
-            a_fy = fma(s0, wxi * W.wf[1][j], a_fy);
-            a_fz = fma(s1, wxi * wyj, a_fz);
-        }
-    }
-    a_pot = warp_sum(a_pot);
-    if (force) {
-        a_fx = warp_sum(a_fx);
-        a_fy = warp_sum(a_fy);
-        a_fz = warp_sum(a_fz);
-    }
-    if (lane == 0) {
-        const int loc = orig - S.part_off;
-        const double scale = S.h3 * S.d;
-        if (force) {
-            const double qs = rc.w / S.d * scale;
-            out[S.out_off + loc] = qs * a_fx;
-            out[S.out_off + loc + S.N] = qs * a_fy;
-            out[S.out_off + loc + 2 * S.N] = qs * a_fz;
-            if (phi_out) phi_out[S.part_off + loc] = scale * a_pot;
-        } else {
-            out[S.out_off + loc] = scale * a_pot;
-        }
-    }
-}
+#include "se_interp.cuh"
 
 // ---------------------------------------------------------------- energy --
 
@@ -670,6 +251,7 @@ struct se_batch_s {
     int max_P = 0;
     bool staged_interp = true;
     size_t interp_smem = 0;
+    int plane = 0;   // x-plane pitch of the staged interpolation window
     // per-stage CUDA events (prepare+sort, spread, k-space, interp)
     bool timing = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -699,10 +281,34 @@ static bool valid_system(const se_system& s)
            s.L > 0 && s.xi > 0 && s.m > 0 && (s.mode == SE_POTENTIAL || s.mode == SE_FORCE);
 }
 
-static size_t interp_smem_bytes(int P, int precision)
+// Pitch between the x planes of the staged interpolation window: at least
+// E * Ep, padded so that the rows one warp reads together (lane l takes row
+// (l / P, l % P)) fall in as few 4-byte banks per wavefront as possible.
+static int interp_plane(int P)
 {
     const int E = FB + P - 1, Ep = E | 1;
-    return (size_t)E * E * Ep * (precision == SE_FP32 ? 4 : 8);
+    int best = E * Ep, best_conf = 1 << 30;
+    for (int pad = 0; pad < 32; pad++) {
+        const int plane = E * Ep + pad;
+        int count[32] = {0};
+        for (int l = 0; l < 32 && l < P * P; l++) {
+            const int i = l / P, j = l % P;
+            count[(i * plane + j * Ep) & 31]++;
+        }
+        int conf = 0;
+        for (int b = 0; b < 32; b++) conf = std::max(conf, count[b]);
+        if (conf < best_conf) {
+            best_conf = conf;
+            best = plane;
+        }
+    }
+    return best;
+}
+
+static size_t interp_smem_bytes(int P, int precision)
+{
+    const int E = FB + P - 1;
+    return (size_t)E * interp_plane(P) * (precision == SE_FP32 ? 4 : 8);
 }
 
 static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nbins_out,
@@ -839,7 +445,8 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     b->nbins = bcur;
     b->ntiles = tcur;
     b->interp_smem = interp_smem_bytes(b->max_P, precision);
-    b->staged_interp = b->interp_smem + sizeof(InterpWarpSmem) * INTERP_WARPS <= 220 * 1024;
+    b->plane = interp_plane(b->max_P);
+    b->staged_interp = b->interp_smem + sizeof(InterpWarpSmem<double>) * INTERP_WARPS <= 220 * 1024;
 
     auto fail = [&](int code) {
         batch_free(b);
@@ -989,7 +596,7 @@ static int launch_interp_staged(se_batch b, const double* grid, double* out, dou
     const dim3 grd(std::max(b->nbins, 1)), blk(INTERP_WARPS * 32);
     const T* fac = static_cast<const T*>(b->fac);
 #define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, fac, b->PS, b->boff, \
-                 grid, out, phi
+                 grid, out, phi, b->plane
     if (uniform && P == 8) k_interp<T, 8><<<grd, blk, smem, st>>>(SE_IARGS);
     else if (uniform && P == 12) k_interp<T, 12><<<grd, blk, smem, st>>>(SE_IARGS);
     else if (uniform && P == 16) k_interp<T, 16><<<grd, blk, smem, st>>>(SE_IARGS);
