@@ -134,6 +134,158 @@ def ncu_traffic():
         return json.load(f)
 
 
+def c3_systems(seed=3):
+    """256 independent POTENTIAL systems: N log-uniform in [1e3, 6.4e4], L in
+    [1, 4], M = 64 (h = L/64), P from {8, 12, 16}, xi = 8/L, charges +-1."""
+    import numpy as np
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for i in range(256):
+        N = int(round(np.exp(rng.uniform(np.log(1e3), np.log(6.4e4)))))
+        L = float(rng.uniform(1.0, 4.0))
+        P = int(rng.choice([8, 12, 16]))
+        out.append(dict(N=N, M=64, P=P, L=L, xi=8.0 / L, seed=1000 + i))
+    return out
+
+
+def run_batched(args):
+    """C3: 256 systems per step, one sort / spread / interpolation launch and
+    one batched cuFFT plan for all of them (FP32 gridding, FP64 k-space)."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from se_fast_gridding_b200 import shard, solver
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    allsys = c3_systems()
+    mine = shard.partition([solver.System(s["N"], s["M"], s["P"], s["L"], s["xi"]) for s in allsys],
+                           world)[rank]
+    systems = [solver.System(allsys[i]["N"], 64, allsys[i]["P"], allsys[i]["L"], allsys[i]["xi"])
+               for i in mine]
+    xs, qs = [], []
+    for i in mine:
+        s = allsys[i]
+        x, q = O.synthetic_system(s["N"], s["L"], seed=s["seed"])
+        xs.append(x)
+        qs.append(q)
+    b = solver.BatchSolver(systems, precision="fp32")
+    x, q = b.pack(xs, qs, device=dev)
+    out = torch.empty(int(b.out_off[-1]), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    b.set_timing(True)
+    for _ in range(args.warmup):
+        b.solve(x, q, out)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ms = []
+    stage = {"sort": [], "spread": [], "kspace": [], "interp": []}
+    launches = 0
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.solve(x, q, out)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        launches += b.launches
+        for kk, v in b.stage_ms().items():
+            stage[kk].append(v)
+    t = sum(ms) / len(ms)
+    if pg:
+        t = shard.max_over_ranks(t)
+    ntot_all = sum(s["N"] for s in allsys)
+    # accuracy of a few systems: FP32 batch vs FP64 single solves
+    errs = []
+    outs = b.split(out)
+    for j in range(min(4, len(systems))):
+        s = systems[j]
+        se = solver.SpectralEwald(s.M, s.P, s.L, s.xi, None, "potential", "fp64", s.N)
+        ref = se.solve(torch.tensor(xs[j], device=dev), torch.tensor(qs[j], device=dev))
+        errs.append(O.rel_rms(outs[j].cpu().numpy(), ref.cpu().numpy()))
+        se.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ntot_all / (t * 1e-3), "unit": "particles/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "C3 batched SE3P POTENTIAL: 256 systems, N log-uniform "
+                                   "[1e3, 6.4e4], L in [1,4], M=64, P in {8,12,16}, xi=8/L, "
+                                   "FP32 gridding, FP64 k-space, one launch set",
+                       "systems": 256, "particles": ntot_all,
+                       "l2": "flushed between steps (256 MiB write)"},
+            "solves_per_s": 256 / (t * 1e-3), "stage_ms": {k: sum(v) / len(v) for k, v in stage.items()},
+            "gpu_launches": launches, "accuracy": {"rel_rms_fp32_vs_fp64_4_systems": max(errs)},
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def run_large(args):
+    """C5: one clustered FORCE system, N = 16M (64 Gaussian clusters of width
+    0.02 L), M = 512^3, P = 12, xi = 60, FP32 gridding, FP64 k-space."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from se_fast_gridding_b200 import solver
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N, M, P, xi = 16_000_000, 512, 12, 60.0
+    x_np, q_np = O.synthetic_system(N, 1.0, seed=5 + rank, charges="pm1", clusters=64, sigma=0.02)
+    x, q = torch.tensor(x_np, device=dev), torch.tensor(q_np, device=dev)
+    se = solver.SpectralEwald(M, P, 1.0, xi, None, "force", "fp32", N)
+    out = torch.empty(3 * N, dtype=torch.float64, device=dev)
+    se.set_timing(True)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(1, args.warmup)):
+        se.solve(x, q, out)
+    ms, stage = [], {"sort": [], "spread": [], "kspace": [], "interp": []}
+    for k in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        se.solve(x, q, out)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        for kk, v in se.stage_ms().items():
+            stage[kk].append(v)
+    t = sum(ms) / len(ms)
+    # accuracy on a 2,000-particle subset: FP32 vs the FP64 path
+    s64 = solver.SpectralEwald(M, P, 1.0, xi, None, "force", "fp64", N)
+    f64 = s64.solve(x, q)
+    idx = torch.arange(0, N, N // 2000, device=dev)[:2000]
+    sub32 = torch.cat([out[idx + d * N] for d in range(3)]).cpu().numpy()
+    sub64 = torch.cat([f64[idx + d * N] for d in range(3)]).cpu().numpy()
+    err = O.rel_rms(sub32, sub64)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": world * N / (t * 1e-3), "unit": "particles/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded clustered)",
+            "config": {"workload": "C5 clustered SE3P FORCE N=16e6 (64 clusters, sigma 0.02 L) "
+                                   "M=512^3 P=12 xi=60, FP32 gridding, FP64 k-space",
+                       "N": N, "M": M, "P": P},
+            "stage_ms": {k: sum(v) / len(v) for k, v in stage.items()},
+            "accuracy": {"rel_rms_fp32_vs_fp64_2000": err},
+        }), flush=True)
+
+
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -169,9 +321,16 @@ def main():
     ap.add_argument("--ref-procs", type=int, default=0,
                     help="CPU processes for --impl reference (default: all cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: the headline single FORCE system; c3: 256 batched systems; "
+                         "c5: 16M clustered particles")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "c3":
+        return run_batched(args)
+    if args.workload == "c5":
+        return run_large(args)
 
     import numpy as np
     import torch

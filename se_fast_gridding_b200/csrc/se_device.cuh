@@ -7,7 +7,32 @@ constexpr int TX = 16, TY = 16, TZ = 16;  // spread tile (output cells)
 constexpr int WY = 4, WZ = 8;             // one warp's lane block: 4 y x 8 z
 constexpr int SPREAD_WARPS = (TY / WY) * (TZ / WZ);
 constexpr int SPREAD_THREADS = SPREAD_WARPS * 32;
-constexpr int CHUNK = 64;                 // particles staged per spread round
+// particles staged per spread round
+template <typename Acc>
+constexpr int spread_chunk() { return 64; }
+
+// Packed FP32 pairs (sm_100a): one fma.rn.f32x2 does two FP32 FMAs.
+__device__ __forceinline__ unsigned long long f32x2(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ float2 f32x2_unpack(unsigned long long v)
+{
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
 constexpr int MAX_SEG = 96;               // bin segments reaching one tile
 constexpr int INTERP_WARPS = 8;
 constexpr int MAX_P = 32;

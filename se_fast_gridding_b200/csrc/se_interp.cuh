@@ -163,6 +163,10 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
                 fz[k] = W.fz[k];
             }
         }
+        // with 32 % P == 0 every row of a lane has the same j = lane % P (the
+        // same test for compile-time and runtime P keeps the arithmetic, and so
+        // the result, of a system identical alone and in a mixed batch)
+        const bool JFIX = (32 % P) == 0;
         double a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
         for (int r = lane; r < P * P; r += 32) {
             const int i = r / P, j = r - (r / P) * P;
@@ -182,14 +186,33 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
                     if (force) s1 = fma(hv, W.fz[k], s1);
                 }
             }
-            const double wxi = W.wx[i], wyj = W.wy[j];
             const double d0 = (double)s0;
-            a_pot = fma(d0, wxi * wyj, a_pot);
-            if (force) {
-                a_fx = fma(d0, W.fx[i] * wyj, a_fx);
-                a_fy = fma(d0, wxi * W.fy[j], a_fy);
-                a_fz = fma((double)s1, wxi * wyj, a_fz);
+            if (JFIX) {   // j is the lane's own: the y weights multiply once below
+                const double wxi = W.wx[i];
+                a_pot = fma(d0, wxi, a_pot);
+                if (force) {
+                    a_fx = fma(d0, W.fx[i], a_fx);
+                    a_fz = fma((double)s1, wxi, a_fz);
+                }
+            } else {
+                const double wxi = W.wx[i], wyj = W.wy[j];
+                a_pot = fma(d0, wxi * wyj, a_pot);
+                if (force) {
+                    a_fx = fma(d0, W.fx[i] * wyj, a_fx);
+                    a_fy = fma(d0, wxi * W.fy[j], a_fy);
+                    a_fz = fma((double)s1, wxi * wyj, a_fz);
+                }
             }
+        }
+        if (JFIX) {
+            const int j = lane % P;
+            const double wyj = W.wy[j];
+            if (force) {
+                a_fy = a_pot * W.fy[j];
+                a_fx *= wyj;
+                a_fz *= wyj;
+            }
+            a_pot *= wyj;
         }
         a_pot = warp_sum(a_pot);
         if (force) {

@@ -281,6 +281,34 @@ static bool valid_system(const se_system& s)
            s.L > 0 && s.xi > 0 && s.m > 0 && (s.mode == SE_POTENTIAL || s.mode == SE_FORCE);
 }
 
+// The per-system fields of the device table that follow from (N, M, P, L,
+// xi, m, mode): stencil offset, bin and tile counts, Gaussian and k-space
+// constants.  Offsets into the batch's arrays are the caller's.
+static void fill_sysdev(const se_system& s, SysDev& S)
+{
+    double h, w, eta, c, d;
+    derive(s.M, s.P, s.L, s.xi, s.m, &h, &w, &eta, &c, &d);
+    const int ph = (s.P & 1) ? (s.P - 1) / 2 : s.P / 2;
+    S.N = s.N;
+    S.M = s.M;
+    S.P = s.P;
+    S.lo = (s.P & 1) ? -ph : -ph + 1;
+    S.mode = s.mode;
+    const int nf = (s.M + FB - 1) / FB;
+    S.nf[0] = S.nf[1] = S.nf[2] = nf;
+    S.nt[0] = (s.M + TX - 1) / TX;
+    S.nt[1] = (s.M + TY - 1) / TY;
+    S.nt[2] = (s.M + TZ - 1) / TZ;
+    S.h = h;
+    S.c = c;
+    S.d = d;
+    S.h3 = h * h * h;
+    S.rho = exp(-2.0 * c * h * h);
+    S.kfac = 2.0 * PI_D / s.L;
+    S.scalar = -(1. - eta) / (4. * s.xi * s.xi);
+    S.dnorm = 4. * PI_D / (double)(s.M * s.M * s.M);
+}
+
 // Pitch between the x planes of the staged interpolation window: at least
 // E * Ep, padded so that the rows one warp reads together (lane l takes row
 // (l / P, l % P)) fall in as few 4-byte banks per wavefront as possible.
@@ -402,33 +430,14 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         const se_system& s = systems[i];
         SysDev& S = b->host_sys[i];
         memset(&S, 0, sizeof(S));
-        double h, w, eta, c, d;
-        derive(s.M, s.P, s.L, s.xi, s.m, &h, &w, &eta, &c, &d);
-        const int ph = (s.P & 1) ? (s.P - 1) / 2 : s.P / 2;
-        S.N = s.N;
-        S.M = s.M;
-        S.P = s.P;
-        S.lo = (s.P & 1) ? -ph : -ph + 1;
-        S.mode = s.mode;
+        fill_sysdev(s, S);
+        const int nf = S.nf[0];
         S.part_off = pcur;
         S.out_off = ocur;
         S.grid_off = goff[i];
         S.spec_off = soff[i];
-        const int nf = (s.M + FB - 1) / FB;
-        S.nf[0] = S.nf[1] = S.nf[2] = nf;
         S.bin_base = bcur;
-        S.nt[0] = (s.M + TX - 1) / TX;
-        S.nt[1] = (s.M + TY - 1) / TY;
-        S.nt[2] = (s.M + TZ - 1) / TZ;
         S.tile_base = tcur;
-        S.h = h;
-        S.c = c;
-        S.d = d;
-        S.h3 = h * h * h;
-        S.rho = exp(-2.0 * c * h * h);
-        S.kfac = 2.0 * PI_D / s.L;
-        S.scalar = -(1. - eta) / (4. * s.xi * s.xi);
-        S.dnorm = 4. * PI_D / (double)(s.M * s.M * s.M);
         b->part_prefix[i] = pcur;
         b->tile_prefix[i] = tcur;
         b->bin_prefix[i] = bcur;
@@ -501,11 +510,25 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
                               g.count);
         if (r != CUFFT_SUCCESS) return fail(cufft_fail(r, "cufftPlanMany"));
     }
+    {
+        // the spread tiles want four CTAs of ~48 KB shared memory per SM
+        const int carve = (int)cudaSharedmemCarveoutMaxShared;
+        cudaError_t a = cudaFuncSetAttribute((const void*)k_spread<float>,
+                                             cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (a == cudaSuccess)
+            a = cudaFuncSetAttribute((const void*)k_spread<double>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
+    }
     if (b->staged_interp) {
         const size_t smem = b->interp_smem;
         auto set = [&](const void* fn) {
-            return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared);
+            return e;
         };
         cudaError_t a = cudaSuccess;
         if (precision == SE_FP32) {

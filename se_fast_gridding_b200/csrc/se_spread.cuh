@@ -4,7 +4,7 @@
 //
 // One CTA owns a TX x TY x TZ tile of one system's periodic grid and visits
 // every particle whose stencil reaches the tile: the particles of at most
-// 7 x 7 x 2 contiguous bin segments, gathered into chunks of CHUNK.  For each
+// 7 x 7 x 2 contiguous bin segments, gathered into chunks of spread_chunk<Acc>().  For each
 // chunk the CTA builds the factor rows of its particles restricted to the
 // tile (px[TX], py[TY], pz[TZ], zero outside the stencil, the charge folded
 // into px) from the precomputed factors, with bit masks of the nonzero y and
@@ -58,26 +58,88 @@ __device__ __forceinline__ int range_at(const BinRanges& r, int k)
 
 template <typename Acc>
 struct SpreadSmem {
-    Acc px[CHUNK][TX];
-    Acc py[CHUNK][TY];
-    Acc pz[CHUNK][TZ];
-    unsigned ymask[CHUNK];
-    unsigned zmask[CHUNK];
-    int pidx[CHUNK];
+    Acc px[spread_chunk<Acc>()][TX];
+    Acc py[spread_chunk<Acc>()][TY];
+    Acc pz[spread_chunk<Acc>()][TZ];
+    unsigned ymask[spread_chunk<Acc>()];
+    unsigned zmask[spread_chunk<Acc>()];
+    int pidx[spread_chunk<Acc>()];
     int seg_beg[SPREAD_THREADS];
     int seg_pre[SPREAD_THREADS];
     int wsum[SPREAD_WARPS];
+    // FP64 fold of the FP32 chunk sums, [cell x][thread] (FP32 path only)
+    double fold[sizeof(Acc) == 4 ? TX : 1][SPREAD_THREADS];
+};
+
+// The TX accumulators of one lane.
+template <typename Acc>
+struct SpreadAccum;
+
+template <>
+struct SpreadAccum<float> {
+    unsigned long long v[TX / 2];   // packed pairs (x = 2m, 2m + 1)
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int m = 0; m < TX / 2; m++) v[m] = 0ull;
+    }
+    __device__ __forceinline__ void add(const float* px, float c)
+    {
+        const unsigned long long cc = f32x2(c, c);
+        const ulonglong2* p2 = reinterpret_cast<const ulonglong2*>(px);
+#pragma unroll
+        for (int m = 0; m < TX / 4; m++) {
+            const ulonglong2 w = p2[m];
+            v[2 * m] = ffma2(w.x, cc, v[2 * m]);
+            v[2 * m + 1] = ffma2(w.y, cc, v[2 * m + 1]);
+        }
+    }
+    __device__ __forceinline__ void fold(SpreadSmem<float>& sm, int t)
+    {
+#pragma unroll
+        for (int m = 0; m < TX / 2; m++) {
+            const float2 f = f32x2_unpack(v[m]);
+            sm.fold[2 * m][t] += (double)f.x;
+            sm.fold[2 * m + 1][t] += (double)f.y;
+            v[m] = 0ull;
+        }
+    }
+    __device__ __forceinline__ double result(const SpreadSmem<float>& sm, int t, int x) const
+    {
+        return sm.fold[x][t];
+    }
+};
+
+template <>
+struct SpreadAccum<double> {
+    double v[TX];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int x = 0; x < TX; x++) v[x] = 0.0;
+    }
+    __device__ __forceinline__ void add(const double* px, double c)
+    {
+#pragma unroll
+        for (int x = 0; x < TX; x++) v[x] = fma(px[x], c, v[x]);
+    }
+    __device__ __forceinline__ void fold(SpreadSmem<double>&, int) {}
+    __device__ __forceinline__ double result(const SpreadSmem<double>&, int, int x) const
+    {
+        return v[x];
+    }
 };
 
 template <typename Acc>
-__global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
+__global__ void __launch_bounds__(SPREAD_THREADS, sizeof(Acc) == 4 ? 4 : 2) k_spread(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const Acc* __restrict__ fac, int PS, const int* __restrict__ boff, double* __restrict__ grid)
 {
     constexpr bool FOLD = sizeof(Acc) == 4;
-    static_assert(TX == 16 && TY == 16 && TZ == 16 && CHUNK == 64 && SPREAD_WARPS == 8,
-                  "the factor-row builder assumes 16-cell rows and 64-particle chunks");
+    static_assert(TX == 16 && TY == 16 && TZ == 16 && SPREAD_WARPS == 8,
+                  "the factor-row builder assumes 16-cell rows");
+    constexpr int CHUNK = spread_chunk<Acc>();
     __shared__ __align__(16) SpreadSmem<Acc> sm;
 
     const int tile = blockIdx.x;
@@ -124,12 +186,12 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
     sm.seg_beg[t] = beg;
     sm.seg_pre[t] = before + incl - len;
 
-    Acc acc[TX];
-    double accd[FOLD ? TX : 1];
-#pragma unroll
-    for (int x = 0; x < TX; x++) acc[x] = Acc(0);
-#pragma unroll
-    for (int x = 0; x < (FOLD ? TX : 1); x++) accd[x] = 0.0;
+    // accumulators: FP32 as 8 packed pairs (fma.rn.f32x2) with the FP64 fold
+    // of the chunk sums in shared memory; FP64 in registers
+    SpreadAccum<Acc> acc;
+    acc.zero();
+    if (FOLD)
+        for (int x = 0; x < TX; x++) sm.fold[x][t] = 0.0;
 
     for (int c0 = 0; c0 < total; c0 += CHUNK) {
         const int n = min(CHUNK, total - c0);
@@ -145,30 +207,45 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
             sm.pidx[t] = sm.seg_beg[lo] + (pos - sm.seg_pre[lo]);
         }
         __syncthreads();
-        // factor rows: warps 2a, 2a+1 build axis a, one lane per particle
-        if (warp < 6) {
-            const int a = warp >> 1, p = t & 63;
+        // factor rows: lane = (particle, quad of 4 cells); a warp instruction
+        // stores 8 particles' rows of one axis as float4-wide quads, the
+        // minimum number of shared-memory wavefronts for the bytes written
+        for (int u = t; u < 3 * 4 * CHUNK; u += SPREAD_THREADS) {
+            const int a = (u >> 2) / CHUNK, p = (u >> 2) - a * CHUNK, x4 = 4 * (u & 3);
+            Acc v[4] = {Acc(0), Acc(0), Acc(0), Acc(0)};
+            unsigned nib = 0;
             if (p < n) {
                 const int part = sm.pidx[p];
                 const int g = g_of(sg[part], a);
                 const int o = a == 0 ? x0 : (a == 1 ? y0 : z0);
                 const Acc* f = fac + ((long long)part * 3 + a) * PS;
-                const Acc scale = a == 0 ? (Acc)srec[part].w : Acc(1);
-                Acc* dst = a == 0 ? sm.px[p] : (a == 1 ? sm.py[p] : sm.pz[p]);
-                unsigned mask = 0;
-                int i = wrap1(o - g, S.M);
+                int k0 = wrap1(o + x4 - g, S.M);
 #pragma unroll
-                for (int xo = 0; xo < 16; xo++) {
-                    Acc v = Acc(0);
-                    if (o + xo < S.M)
-                        for (int k = i; k < S.P; k += S.M) v += f[k];
-                    dst[xo] = v * scale;
-                    mask |= (v != Acc(0)) ? (1u << xo) : 0u;
-                    if (++i >= S.M) i -= S.M;
+                for (int e = 0; e < 4; e++) {
+                    if (o + x4 + e < S.M)
+                        for (int k = k0; k < S.P; k += S.M) v[e] += f[k];
+                    if (++k0 >= S.M) k0 -= S.M;
                 }
-                if (a == 1) sm.ymask[p] = mask;
-                if (a == 2) sm.zmask[p] = mask;
+                if (a == 0) {
+                    const Acc qw = (Acc)srec[part].w;
+#pragma unroll
+                    for (int e = 0; e < 4; e++) v[e] *= qw;
+                }
+#pragma unroll
+                for (int e = 0; e < 4; e++) nib |= (v[e] != Acc(0)) ? (1u << e) : 0u;
+                Acc* row = (a == 0 ? sm.px[p] : (a == 1 ? sm.py[p] : sm.pz[p])) + x4;
+                if constexpr (sizeof(Acc) == 4) {
+                    *reinterpret_cast<float4*>(row) = make_float4(v[0], v[1], v[2], v[3]);
+                } else {
+                    reinterpret_cast<double2*>(row)[0] = make_double2(v[0], v[1]);
+                    reinterpret_cast<double2*>(row)[1] = make_double2(v[2], v[3]);
+                }
             }
+            // 16-bit row mask of the particle from the four lanes of its quads
+            unsigned m = nib << x4;
+            m |= __shfl_xor_sync(0xffffffffu, m, 1);
+            m |= __shfl_xor_sync(0xffffffffu, m, 2);
+            if (a > 0 && x4 == 0 && p < n) (a == 1 ? sm.ymask : sm.zmask)[p] = m;
         }
         __syncthreads();
         // this warp's particles: the stencil meets its (y, z) lane block
@@ -179,29 +256,20 @@ __global__ void __launch_bounds__(SPREAD_THREADS) k_spread(
             while (bits) {
                 const int p = base + __ffs(bits) - 1;
                 bits &= bits - 1;
-                const Acc c = sm.py[p][ly] * sm.pz[p][lz];
-                const Acc* px = sm.px[p];
-#pragma unroll
-                for (int x = 0; x < TX; x++) acc[x] = fma(px[x], c, acc[x]);
+                acc.add(sm.px[p], sm.py[p][ly] * sm.pz[p][lz]);
             }
         }
-        if (FOLD) {
-#pragma unroll
-            for (int x = 0; x < TX; x++) {
-                accd[x] += (double)acc[x];
-                acc[x] = Acc(0);
-            }
-        }
+        if (FOLD) acc.fold(sm, t);
     }
 
     // ---- write the tile (every cell once; cells past M belong to no tile)
+    if (FOLD) __syncwarp();
     const int gy = y0 + ly, gz = z0 + lz;
     if (gy >= S.M || gz >= S.M) return;
     double* gs = grid + S.grid_off;
 #pragma unroll
     for (int x = 0; x < TX; x++) {
         const int gx = x0 + x;
-        if (gx < S.M)
-            gs[((long long)gx * S.M + gy) * S.M + gz] = FOLD ? accd[x] : (double)acc[x];
+        if (gx < S.M) gs[((long long)gx * S.M + gy) * S.M + gz] = acc.result(sm, t, x);
     }
 }
