@@ -117,6 +117,23 @@ size_t se_sort_scratch_bytes(int N, int nkeys);
 int se_counting_sort(const int* keys, int N, int nkeys, int* perm, int* offsets,
                      void* scratch, size_t scratch_bytes, void* stream);
 
+/* The same sort for callers that cannot allocate device memory when they
+ * sort (a frozen or captured memory pool, host callbacks, real-time loops, a
+ * library that does not own the process's allocator).  No counterpart in the
+ * reference.  It allocates nothing: its working memory is a device array of
+ * SE_SORT_STATIC_BYTES inside the library (held on every GPU that loads the
+ * library, until exit), so N <= SE_SORT_STATIC_MAX_N and
+ * nkeys <= SE_SORT_STATIC_MAX_KEYS; larger sizes return SE_ERR_INVALID.
+ * The first call on a device resolves the array's address and should come
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller.  Results are identical
+ * to se_counting_sort. */
+#define SE_SORT_STATIC_MAX_N 262144
+#define SE_SORT_STATIC_MAX_KEYS 65536
+#define SE_SORT_STATIC_BYTES (6u << 20)
+int se_counting_sort_static(const int* keys, int N, int nkeys, int* perm, int* offsets,
+                            void* stream);
+
 /* ---------------------------------------------------------------- batch -- */
 /* Many independent systems solved together: one sort, one spread launch and
  * one interpolation launch over all systems through per-system offset
