@@ -44,7 +44,9 @@ enum {
     SE_ERR_UNSUPPORTED = 3,
     SE_ERR_NOMEM = 4,
     SE_ERR_CUFFT = 5,
-    SE_ERR_INPUT = 6     /* a position was not finite */
+    SE_ERR_INPUT = 6,    /* a position was not finite */
+    SE_ERR_BUSY = 7,     /* a server's queue is full */
+    SE_ERR_TIMEOUT = 8   /* a wait on a server ran out */
 };
 
 enum { SE_POTENTIAL = 0, SE_FORCE = 1 };
@@ -160,6 +162,77 @@ int se_batch_solve(se_batch batch, const double* x, const double* q, double* out
 int se_batch_launch_count(se_batch batch);
 int se_batch_set_timing(se_batch batch, int on);
 int se_batch_stage_ms(se_batch batch, float ms[4]);
+
+/* Solve one system on a plan made for the same M, P and mode, with the
+ * system's own N (<= the plan's max_particles), L, xi and m.  The plan's
+ * device table is rewritten in stream order, so a plan kept per (M, P, mode)
+ * serves systems of any box size and particle count without a host wait.
+ * Results are identical to a plan created for exactly this system. */
+int se_solve_system(se_plan plan, const se_system* sys, const double* x, const double* q,
+                    double* out, double* phi_out, void* stream);
+
+/* -------------------------------------------------------------- serving -- */
+/* A request loop on the current GPU (no counterpart in the reference).
+ * Requests are queued as they arrive and admitted first come, first served
+ * whenever a solve slot (a CUDA stream) is free and the plan the request
+ * needs fits the device-memory budget.  Plans (grid, spectrum, particle and
+ * staging buffers, cuFFT plans) are cached by (M, P, mode, capacity class) and
+ * stay resident between requests; an idle plan is freed, least recently used
+ * first, only when a new one would not otherwise fit.  Admitted solves run on
+ * their own streams and overlap on the device, so requests that arrive while
+ * others are running start as soon as a slot and memory are free.  Each
+ * result is bit-identical to se_solve_system on the same inputs, alone or in
+ * any mix.  Host requests should use pinned memory: a copy from or to
+ * pageable memory makes the loop wait for it. */
+#define SE_WHERE_HOST 0     /* x, q, out are host memory */
+#define SE_WHERE_DEVICE 1   /* x, q, out are device memory on the server's GPU */
+
+typedef struct {
+    int slots;          /* solves in flight at once, 1..64                     */
+    int precision;      /* SE_FP32 or SE_FP64 gridding                         */
+    size_t hbm_budget;  /* device bytes the server may hold (plans + staging)  */
+    int max_queue;      /* queued requests before submit says SE_ERR_BUSY; 0: no limit */
+} se_server_config;
+
+typedef struct {
+    se_system sys;      /* N, M, P, L, xi, m, mode                             */
+    const double* x;    /* 3N positions, SoA; valid until the request completes */
+    const double* q;    /* N charges                                           */
+    double* out;        /* N potentials (POTENTIAL) or 3N forces, SoA (FORCE)  */
+    int where;          /* SE_WHERE_HOST or SE_WHERE_DEVICE                    */
+} se_request;
+
+typedef struct {
+    long long ticket;
+    int status;         /* SE_OK, SE_ERR_INPUT (a position was not finite), ... */
+    double queue_s;     /* submit to admission                                 */
+    double latency_s;   /* submit to result in place                           */
+} se_completion;
+
+typedef struct {
+    long long submitted, completed, failed;
+    int queued, in_flight, plans;
+    long long plans_created, plans_evicted;
+    size_t hbm_used, hbm_peak;
+} se_server_stats;
+
+typedef struct se_server_s* se_server;
+
+/* Device bytes the server charges for a request's plan (admission unit). */
+size_t se_server_request_bytes(const se_system* sys, int precision);
+int se_server_create(se_server* server, const se_server_config* cfg);
+/* Builds and caches plans for these systems now (a warm cache). */
+int se_server_reserve(se_server server, const se_system* systems, int n);
+/* Queues a request; SE_ERR_NOMEM if its plan alone exceeds the budget. */
+int se_server_submit(se_server server, const se_request* req, long long* ticket);
+/* Moves up to max completions (in completion order) into done, no waiting. */
+int se_server_poll(se_server server, se_completion* done, int max, int* n_done);
+/* Waits until every submitted request has completed (SE_ERR_TIMEOUT after
+ * timeout_s seconds; a negative timeout waits without limit). */
+int se_server_drain(se_server server, double timeout_s);
+int se_server_get_stats(se_server server, se_server_stats* stats);
+/* Drains, then frees every plan, stream and buffer. */
+int se_server_destroy(se_server server);
 
 #ifdef __cplusplus
 }

@@ -57,13 +57,42 @@ class se_system(C.Structure):
                 ("xi", C.c_double), ("m", C.c_double), ("mode", C.c_int)]
 
 
+class se_server_config(C.Structure):
+    """se_gpu.h se_server_config."""
+    _fields_ = [("slots", C.c_int), ("precision", C.c_int), ("hbm_budget", C.c_size_t),
+                ("max_queue", C.c_int)]
+
+
+class se_request(C.Structure):
+    """se_gpu.h se_request."""
+    _fields_ = [("sys", se_system), ("x", C.c_void_p), ("q", C.c_void_p), ("out", C.c_void_p),
+                ("where", C.c_int)]
+
+
+class se_completion(C.Structure):
+    """se_gpu.h se_completion."""
+    _fields_ = [("ticket", C.c_longlong), ("status", C.c_int), ("queue_s", C.c_double),
+                ("latency_s", C.c_double)]
+
+
+class se_server_stats(C.Structure):
+    """se_gpu.h se_server_stats."""
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("failed", C.c_longlong), ("queued", C.c_int), ("in_flight", C.c_int),
+                ("plans", C.c_int), ("plans_created", C.c_longlong),
+                ("plans_evicted", C.c_longlong), ("hbm_used", C.c_size_t),
+                ("hbm_peak", C.c_size_t)]
+
+
 SE_OK, SE_ERR_CUDA, SE_ERR_INVALID, SE_ERR_UNSUPPORTED, SE_ERR_NOMEM, SE_ERR_CUFFT, \
-    SE_ERR_INPUT = range(7)
+    SE_ERR_INPUT, SE_ERR_BUSY, SE_ERR_TIMEOUT = range(9)
+SE_WHERE_HOST, SE_WHERE_DEVICE = 0, 1
 SE_POTENTIAL, SE_FORCE = 0, 1
 SE_FP64, SE_FP32 = 0, 1
 
 _ERR_NAMES = {1: "CUDA error", 2: "invalid argument", 3: "unsupported", 4: "out of memory",
-              5: "cuFFT error", 6: "non-finite position"}
+              5: "cuFFT error", 6: "non-finite position", 7: "queue full",
+              8: "timed out"}
 
 
 class SEError(RuntimeError):
@@ -113,6 +142,16 @@ def lib() -> C.CDLL:
         "se_batch_set_timing": (C.c_int, [_vp, C.c_int]),
         "se_batch_stage_ms": (C.c_int, [_vp, C.POINTER(C.c_float * 4)]),
         "se_probe_fma_tflops": (C.c_int, [_dp, _vp]),
+        "se_solve_system": (C.c_int, [_vp, C.POINTER(se_system), _vp, _vp, _vp, _vp, _vp]),
+        "se_server_request_bytes": (C.c_size_t, [C.POINTER(se_system), C.c_int]),
+        "se_server_create": (C.c_int, [C.POINTER(_vp), C.POINTER(se_server_config)]),
+        "se_server_reserve": (C.c_int, [_vp, C.POINTER(se_system), C.c_int]),
+        "se_server_submit": (C.c_int, [_vp, C.POINTER(se_request), C.POINTER(C.c_longlong)]),
+        "se_server_poll": (C.c_int, [_vp, C.POINTER(se_completion), C.c_int,
+                                     C.POINTER(C.c_int)]),
+        "se_server_drain": (C.c_int, [_vp, C.c_double]),
+        "se_server_get_stats": (C.c_int, [_vp, C.POINTER(se_server_stats)]),
+        "se_server_destroy": (C.c_int, [_vp]),
         # legacy helpers with return values
         "SE_gettime": (C.c_double, []),
         "SE_prod3": (C.c_int, [C.POINTER(C.c_int * 3)]),

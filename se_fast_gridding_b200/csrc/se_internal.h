@@ -39,6 +39,10 @@ int stable_sort(const int* keys, const int* vals_in, int N, int nkeys, int* perm
                 int* sorted_keys, int* offsets, void* scratch, size_t scratch_bytes,
                 cudaStream_t st, int* launches);
 
+// Device flag a plan's kernels set when a position was not finite (reset at
+// the start of each solve on the plan's stream).
+const int* plan_error_flag(se_plan p);
+
 // exclusive scan of n ints (in place allowed), total written to out[n] if
 // write_total; scratch of scan_scratch_bytes(n)
 size_t scan_scratch_bytes(long n);

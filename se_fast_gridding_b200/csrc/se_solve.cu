@@ -248,6 +248,7 @@ struct se_batch_s {
     double* energy_partial = nullptr;
     int* err = nullptr;
     int launches = 0;
+    int pending_launches = 0;   // issued before the next solve's own launches (rebind)
     int max_P = 0;
     bool staged_interp = true;
     size_t interp_smem = 0;
@@ -386,6 +387,52 @@ static int batch_free(se_batch b)
     return SE_OK;
 }
 
+// The staged interpolation kernel a batch launches: specialised on P when
+// every system has the same P in {8, 12, 16} (or 21 in FP64), else generic.
+template <typename T>
+static const void* staged_interp_variant(int P, bool uniform)
+{
+    if (uniform && P == 8) return (const void*)k_interp<T, 8>;
+    if (uniform && P == 12) return (const void*)k_interp<T, 12>;
+    if (uniform && P == 16) return (const void*)k_interp<T, 16>;
+    if (sizeof(T) == 8 && uniform && P == 21) return (const void*)k_interp<T, 21>;
+    return (const void*)k_interp<T, 0>;
+}
+
+static bool uniform_P(const se_batch_s* b)
+{
+    for (auto& s : b->host_sys)
+        if (s.P != b->max_P) return false;
+    return true;
+}
+
+static const void* staged_interp_kernel(const se_batch_s* b)
+{
+    return b->precision == SE_FP32 ? staged_interp_variant<float>(b->max_P, uniform_P(b))
+                                   : staged_interp_variant<double>(b->max_P, uniform_P(b));
+}
+
+// Dynamic shared memory a kernel may use is a per-device, per-function
+// attribute shared by every plan in the process: only ever raise it, so a
+// plan made later with a smaller window cannot break an earlier one.
+static cudaError_t raise_smem_limit(const void* fn, size_t smem)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    size_t& cur = limit[{dev, fn}];
+    if (cur >= smem) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) cur = smem;
+    return e;
+}
+
 static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision)
 {
     if (!out || !systems || nsys < 1 || (precision != SE_FP64 && precision != SE_FP32))
@@ -521,28 +568,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
     }
     if (b->staged_interp) {
-        const size_t smem = b->interp_smem;
-        auto set = [&](const void* fn) {
-            cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
-            if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         (int)cudaSharedmemCarveoutMaxShared);
-            return e;
-        };
-        cudaError_t a = cudaSuccess;
-        if (precision == SE_FP32) {
-            a = set((const void*)k_interp<float, 0>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<float, 8>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<float, 12>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<float, 16>);
-        } else {
-            a = set((const void*)k_interp<double, 0>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<double, 8>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<double, 12>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<double, 16>);
-            if (a == cudaSuccess) a = set((const void*)k_interp<double, 21>);
-        }
+        const cudaError_t a = raise_smem_limit(staged_interp_kernel(b), b->interp_smem);
         if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
     }
     *out = b;
@@ -614,8 +640,7 @@ static int launch_interp_staged(se_batch b, const double* grid, double* out, dou
 {
     const size_t smem = b->interp_smem;
     const int P = b->max_P;
-    bool uniform = true;
-    for (auto& s : b->host_sys) uniform = uniform && s.P == P;
+    const bool uniform = uniform_P(b);
     const dim3 grd(std::max(b->nbins, 1)), blk(INTERP_WARPS * 32);
     const T* fac = static_cast<const T*>(b->fac);
 #define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, fac, b->PS, b->boff, \
@@ -671,7 +696,8 @@ static int run_interp(se_batch b, const double* grid, double* out, double* phi, 
 static int batch_solve(se_batch b, const double* x, const double* q, double* out, double* phi,
                        cudaStream_t st)
 {
-    b->launches = 0;
+    b->launches = b->pending_launches;
+    b->pending_launches = 0;
     auto mark = [&](int i) -> int {
         if (b->timing) SE_CUDA(cudaEventRecord(b->ev[i], st));
         return SE_OK;
@@ -730,7 +756,6 @@ __global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters, float 
 struct se_plan_s {
     se_config cfg;
     se_batch b = nullptr;
-    int N = -1;
     double* h_x = nullptr;   // pinned staging for se_solve_host
     double* h_q = nullptr;
     double* h_out = nullptr;
@@ -782,7 +807,6 @@ extern "C" int se_plan_create(se_plan* plan, const se_config* cfg)
         delete p;
         return r;
     }
-    p->N = cfg->max_particles;
     *plan = p;
     return SE_OK;
 }
@@ -801,21 +825,41 @@ extern "C" int se_plan_destroy(se_plan p)
     return SE_OK;
 }
 
-// Re-point the single-system table at N particles (only when N changes).
+// Stream-ordered rewrite of a single-system plan's device table: the
+// kernels that follow on the stream see the new system, earlier ones the old.
+__global__ void k_rebind(SysDev* sys, int* part_prefix, SysDev s)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *sys = s;
+        part_prefix[1] = s.N;
+    }
+}
+
+// Point a single-system plan at system s (same M, P and mode, N within the
+// plan's capacity; L, xi, m and N free).  Nothing is issued when s is the
+// system the plan already holds.
+static int plan_rebind(se_plan p, const se_system& s, cudaStream_t st)
+{
+    if (!valid_system(s) || s.N > p->cfg.max_particles || s.M != p->cfg.M || s.P != p->cfg.P ||
+        s.mode != p->cfg.mode)
+        return SE_ERR_INVALID;
+    se_batch b = p->b;
+    SysDev S = b->host_sys[0];
+    fill_sysdev(s, S);
+    if (memcmp(&S, &b->host_sys[0], sizeof(S)) == 0) return SE_OK;
+    k_rebind<<<1, 32, 0, st>>>(b->sys, b->d_part_prefix, S);
+    SE_CUDA(cudaGetLastError());
+    b->pending_launches++;
+    b->host_sys[0] = S;
+    b->part_prefix[1] = s.N;
+    b->ntot = s.N;
+    return SE_OK;
+}
+
 static int plan_set_N(se_plan p, int N, cudaStream_t st)
 {
     if (N < 0 || N > p->cfg.max_particles) return SE_ERR_INVALID;
-    if (N == p->N) return SE_OK;
-    se_batch b = p->b;
-    SE_CUDA(cudaStreamSynchronize(st));
-    b->host_sys[0].N = N;
-    b->part_prefix[1] = N;
-    b->ntot = N;
-    SE_CUDA(cudaMemcpy(b->sys, b->host_sys.data(), sizeof(SysDev), cudaMemcpyHostToDevice));
-    SE_CUDA(cudaMemcpy(b->d_part_prefix, b->part_prefix.data(), sizeof(int) * 2,
-                       cudaMemcpyHostToDevice));
-    p->N = N;
-    return SE_OK;
+    return plan_rebind(p, sys_of(&p->cfg, N), st);
 }
 
 extern "C" int se_solve(se_plan p, int N, const double* x, const double* q, double* out,
@@ -824,6 +868,17 @@ extern "C" int se_solve(se_plan p, int N, const double* x, const double* q, doub
     if (!p || (N > 0 && (!x || !q || !out))) return SE_ERR_INVALID;
     cudaStream_t st = as_stream(stream);
     SE_TRY(plan_set_N(p, N, st));
+    return batch_solve(p->b, x, q, out, phi_out, st);
+}
+
+const int* se::plan_error_flag(se_plan p) { return p ? p->b->err : nullptr; }
+
+extern "C" int se_solve_system(se_plan p, const se_system* sys, const double* x,
+                               const double* q, double* out, double* phi_out, void* stream)
+{
+    if (!p || !sys || (sys->N > 0 && (!x || !q || !out))) return SE_ERR_INVALID;
+    cudaStream_t st = as_stream(stream);
+    SE_TRY(plan_rebind(p, *sys, st));
     return batch_solve(p->b, x, q, out, phi_out, st);
 }
 
@@ -856,7 +911,8 @@ extern "C" int se_spread(se_plan p, int N, const double* x, const double* q, dou
     if (!p || !grid || (N > 0 && (!x || !q))) return SE_ERR_INVALID;
     cudaStream_t st = as_stream(stream);
     SE_TRY(plan_set_N(p, N, st));
-    p->b->launches = 0;
+    p->b->launches = p->b->pending_launches;
+    p->b->pending_launches = 0;
     SE_TRY(run_prepare_sort(p->b, x, q, st));
     return run_spread(p->b, grid, st);
 }
@@ -873,7 +929,8 @@ extern "C" int se_interp(se_plan p, int N, const double* x, const double* q, con
     if (!p || !grid || (N > 0 && (!x || !q || !out))) return SE_ERR_INVALID;
     cudaStream_t st = as_stream(stream);
     SE_TRY(plan_set_N(p, N, st));
-    p->b->launches = 0;
+    p->b->launches = p->b->pending_launches;
+    p->b->pending_launches = 0;
     SE_TRY(run_prepare_sort(p->b, x, q, st));
     return run_interp(p->b, grid, out, phi_out, st);
 }

@@ -107,6 +107,20 @@ class SpectralEwald:
                              _stream(stream)), "se_solve")
         return out
 
+    def solve_system(self, system: "System", x: torch.Tensor, q: torch.Tensor,
+                     out: torch.Tensor | None = None, phi_out: torch.Tensor | None = None,
+                     stream=None) -> torch.Tensor:
+        """Solve `system` (same M, P and mode as the plan; its own N, L, xi,
+        m) on this plan (se_solve_system)."""
+        if x.numel() != 3 * system.N or q.numel() != system.N:
+            raise ValueError("x, q sizes do not match system.N")
+        if out is None:
+            out = torch.empty(self.out_width * system.N, dtype=torch.float64, device=q.device)
+        s = system.c_struct()
+        check(lib().se_solve_system(self._plan, C.byref(s), _ptr(x), _ptr(q), _ptr(out),
+                                    _ptr(phi_out), _stream(stream)), "se_solve_system")
+        return out
+
     def solve_host(self, x: np.ndarray, q: np.ndarray, out: np.ndarray | None = None,
                    stream=None) -> np.ndarray:
         """Host buffers in and out (copies inside, waits for the result)."""

@@ -206,6 +206,24 @@ def test_batch_equals_single_systems(S):
                 assert rel(host(o), ref) < FP64_TOL
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_plans_of_different_P_coexist(S, prec):
+    """A plan created later with a smaller interpolation window must not
+    break an earlier plan's launches (per-function launch limits are
+    process-wide)."""
+    import oracle as O
+    x, q = O.synthetic_system(3000, 1.0, seed=31)
+    xd, qd = cuda(x), cuda(q)
+    big = S.SpectralEwald(32, 16, 1.0, 8.0, None, "force", prec, 3000)
+    first = host(big.solve(xd, qd))
+    small = [S.SpectralEwald(32, P, 1.0, 8.0, None, "force", prec, 3000) for P in (8, 12, 4)]
+    for s in small:
+        s.solve(xd, qd)
+    np.testing.assert_array_equal(host(big.solve(xd, qd)), first)
+    for s in small + [big]:
+        s.close()
+
+
 def test_energy(S):
     import torch
     rng = np.random.Generator(np.random.Philox(8))
