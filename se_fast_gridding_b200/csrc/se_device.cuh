@@ -33,6 +33,13 @@ __device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsign
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
     return d;
 }
+// A system's spread runs in k_spread2 (tile-aligned factor rows) when its
+// grid is cut into whole 16^3 tiles and its stencil fits two tiles.
+__host__ __device__ inline bool spread2_eligible(int M, int P)
+{
+    return M % 16 == 0 && M >= 32 && P <= 16;
+}
+
 constexpr int MAX_SEG = 96;               // bin segments reaching one tile
 constexpr int INTERP_WARPS = 8;
 constexpr int MAX_P = 32;

@@ -107,35 +107,75 @@ __global__ void k_gather(int ntot, const int* __restrict__ perm, const double4* 
 
 // ------------------------------------------------------- factor rows -----
 
-// Each particle's separable Gaussian factors, once per solve, in bin order:
-// fac[(s*3 + a)*PS + i] = exp(-c (t0_a - (lo+i) h)^2), i < P, built with the
-// FGG recurrence in FP64 (SE_fgg.c:575-609 restated for the full Gaussian):
-// v_0 = exp(-c u_0^2), r_0 = exp(2 c h u_0 - c h^2), v_{i+1} = v_i r_i,
-// r_{i+1} = r_i exp(-2 c h^2), u_0 = t0 - lo h.  Stored in the working
-// precision T; PS is the batch's largest P.
+// Each particle's separable Gaussian factors, once per solve, in bin order,
+// built with the FGG recurrence in FP64 (SE_fgg.c:575-609 restated for the
+// full Gaussian): v_0 = exp(-c u_0^2), r_0 = exp(2 c h u_0 - c h^2),
+// v_{i+1} = v_i r_i, r_{i+1} = r_i exp(-2 c h^2), u_0 = t0 - lo h, stored in
+// the working precision T.  Thread u = 3 s + a writes particle s, axis a:
+//  - systems k_spread2 serves (spread2_eligible): the tile-aligned 32-entry
+//    row rows[u*32 + j] = f[j - (g_a mod 16)], zero outside the stencil; the
+//    rows of a warp are contiguous, so they are staged in shared memory and
+//    stored as one coalesced block;
+//  - the others: fac[u*PS + i] = f[i], i < P (PS = the batch's largest P).
 template <typename T>
-__global__ void k_factors(const SysDev* __restrict__ sys, const int* __restrict__ part_prefix,
-                          int nsys, int ntot, const double4* __restrict__ srec,
-                          const int* __restrict__ sperm, T* __restrict__ fac, int PS)
+constexpr int factors_threads() { return sizeof(T) == 4 ? 256 : 128; }
+
+template <typename T>
+__global__ void __launch_bounds__(factors_threads<T>()) k_factors(
+    const SysDev* __restrict__ sys, const int* __restrict__ part_prefix, int nsys, int ntot,
+    const double4* __restrict__ srec, const int* __restrict__ sperm, const int* __restrict__ sg,
+    T* __restrict__ fac, int PS, T* __restrict__ rows)
 {
+    constexpr int V = 16 / sizeof(T);   // elements per 16 bytes
+    constexpr int RS = 32 + V;          // staged row pitch, 16-byte aligned
+    __shared__ __align__(16) T stage[factors_threads<T>()][RS];
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= 3 * ntot) return;
-    const int s = u / 3, a = u - 3 * (u / 3);
-    const SysDev& S = sys[find_sys(part_prefix, nsys, sperm[s])];
-    const double4 rc = srec[s];
-    const double t0 = a == 0 ? rc.x : (a == 1 ? rc.y : rc.z);
-    const double u0 = t0 - S.lo * S.h;
-    double v = exp(-S.c * u0 * u0);
-    double r = exp(2.0 * S.c * S.h * u0 - S.c * S.h * S.h);
-    T* f = fac + ((long long)s * 3 + a) * PS;
-    for (int i = 0; i < S.P; i++) {
-        f[i] = (T)v;
-        v *= r;
-        r *= S.rho;
+    const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
+    bool staged = false;
+    if (u < 3 * ntot) {
+        const int s = u / 3, a = u - 3 * (u / 3);
+        const SysDev& S = sys[find_sys(part_prefix, nsys, sperm[s])];
+        const double4 rc = srec[s];
+        const double t0 = a == 0 ? rc.x : (a == 1 ? rc.y : rc.z);
+        const double u0 = t0 - S.lo * S.h;
+        double v = exp(-S.c * u0 * u0);
+        double r = exp(2.0 * S.c * S.h * u0 - S.c * S.h * S.h);
+        if (rows && spread2_eligible(S.M, S.P)) {
+            staged = true;
+            T* st = stage[threadIdx.x];
+#pragma unroll
+            for (int j = 0; j < 32; j += V)
+                *reinterpret_cast<uint4*>(st + j) = make_uint4(0u, 0u, 0u, 0u);
+            st += ((unsigned)sg[s] >> (10 * a)) & 15u;
+            for (int i = 0; i < S.P; i++) {
+                st[i] = (T)v;
+                v *= r;
+                r *= S.rho;
+            }
+        } else {
+            T* f = fac + (long long)u * PS;
+            for (int i = 0; i < S.P; i++) {
+                f[i] = (T)v;
+                v *= r;
+                r *= S.rho;
+            }
+        }
+    }
+    const unsigned srows = __ballot_sync(0xffffffffu, staged);
+    if (!srows) return;
+    __syncwarp();
+    // the warp's 32 rows are rows[(u_w + k) * 32 ...], k < 32: one block
+    const long long uw = (long long)blockIdx.x * blockDim.x + wbase;
+    for (int k = lane; k < 32 * 32 / V; k += 32) {
+        const int r = k / (32 / V), c = (k % (32 / V)) * V;
+        if ((srows >> r) & 1u)
+            *reinterpret_cast<uint4*>(rows + (uw + r) * 32 + c) =
+                *reinterpret_cast<const uint4*>(&stage[wbase + r][c]);
     }
 }
 
 #include "se_spread.cuh"
+#include "se_spread2.cuh"
 
 // --------------------------------------------------------------- k-space --
 
@@ -241,6 +281,8 @@ struct se_batch_s {
     int* boff = nullptr;
     void* fac = nullptr;      // per-particle factors [ntot][3][PS], working precision
     int PS = 0;
+    void* rows = nullptr;     // tile-aligned rows [ntot][3][32] (k_spread2 systems)
+    bool any_spread1 = false, any_spread2 = false;
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     double* grid = nullptr;
@@ -359,7 +401,13 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     b += (size_t)ntot * (4 + 32 + 4 + 4 + 32 + 4);
     int maxP = 1;
     for (int i = 0; i < nsys; i++) maxP = std::max(maxP, sys[i].P);
-    b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
+    bool rows = false, plain = false;
+    for (int i = 0; i < nsys; i++) {
+        if (spread2_eligible(sys[i].M, sys[i].P)) rows = true;
+        else plain = true;
+    }
+    if (plain) b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
+    if (rows) b += (size_t)ntot * 3 * 32 * (precision == SE_FP32 ? 4 : 8);
     b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
     b += (size_t)(nbins + 1) * 4;
     b += (size_t)grid * 8 + (size_t)spec * 16;
@@ -380,7 +428,7 @@ static int batch_free(se_batch b)
         if (e) cudaEventDestroy(e);
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
-                    b->grid, b->spec, b->energy_partial, b->err, b->fac};
+                    b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -526,7 +574,12 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     SE_ALLOC(b->sg, sizeof(int) * nt);
     SE_ALLOC(b->boff, sizeof(int) * (b->nbins + 1));
     b->PS = b->max_P;
-    SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
+    for (int i = 0; i < nsys; i++) {
+        if (spread2_eligible(systems[i].M, systems[i].P)) b->any_spread2 = true;
+        else b->any_spread1 = true;
+    }
+    if (b->any_spread1) SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
+    if (b->any_spread2) SE_ALLOC(b->rows, nt * 3 * 32 * (precision == SE_FP32 ? 4 : 8));
     b->sort_bytes = sort_scratch_bytes(b->ntot, std::max(b->nbins, 1));
     SE_ALLOC(b->sort_scratch, b->sort_bytes);
     SE_ALLOC(b->grid, sizeof(double) * b->grid_elems);
@@ -565,6 +618,12 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         if (a == cudaSuccess)
             a = cudaFuncSetAttribute((const void*)k_spread<double>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (a == cudaSuccess)
+            a = cudaFuncSetAttribute((const void*)k_spread2<float>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (a == cudaSuccess)
+            a = cudaFuncSetAttribute((const void*)k_spread2<double>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
     }
     if (b->staged_interp) {
@@ -601,16 +660,31 @@ static int run_prepare_sort(se_batch b, const double* x, const double* q, cudaSt
 
 static int run_spread(se_batch b, double* grid, cudaStream_t st)
 {
-    if (b->precision == SE_FP32)
-        k_spread<float><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
-            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg, static_cast<const float*>(b->fac),
-            b->PS, b->boff, grid);
-    else
-        k_spread<double><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
-            b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
-            static_cast<const double*>(b->fac), b->PS, b->boff, grid);
-    SE_CUDA(cudaGetLastError());
-    LAUNCHED(b);
+    // every tile is written by exactly one of the two kernels (by system)
+    if (b->any_spread2) {
+        if (b->precision == SE_FP32)
+            k_spread2<float><<<b->ntiles, S2_THREADS, 0, st>>>(
+                b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
+                static_cast<const float*>(b->rows), b->boff, grid);
+        else
+            k_spread2<double><<<b->ntiles, S2_THREADS, 0, st>>>(
+                b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
+                static_cast<const double*>(b->rows), b->boff, grid);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
+    }
+    if (b->any_spread1) {
+        if (b->precision == SE_FP32)
+            k_spread<float><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
+                b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
+                static_cast<const float*>(b->fac), b->PS, b->boff, grid);
+        else
+            k_spread<double><<<b->ntiles, SPREAD_THREADS, 0, st>>>(
+                b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
+                static_cast<const double*>(b->fac), b->PS, b->boff, grid);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
+    }
     return SE_OK;
 }
 
@@ -643,8 +717,9 @@ static int launch_interp_staged(se_batch b, const double* grid, double* out, dou
     const bool uniform = uniform_P(b);
     const dim3 grd(std::max(b->nbins, 1)), blk(INTERP_WARPS * 32);
     const T* fac = static_cast<const T*>(b->fac);
-#define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, fac, b->PS, b->boff, \
-                 grid, out, phi, b->plane
+    const T* rows = static_cast<const T*>(b->rows);
+#define SE_IARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, fac, b->PS, rows, \
+                 b->boff, grid, out, phi, b->plane
     if (uniform && P == 8) k_interp<T, 8><<<grd, blk, smem, st>>>(SE_IARGS);
     else if (uniform && P == 12) k_interp<T, 12><<<grd, blk, smem, st>>>(SE_IARGS);
     else if (uniform && P == 16) k_interp<T, 16><<<grd, blk, smem, st>>>(SE_IARGS);
@@ -659,14 +734,16 @@ static int launch_interp_staged(se_batch b, const double* grid, double* out, dou
 static int run_factors(se_batch b, cudaStream_t st)
 {
     if (b->ntot == 0) return SE_OK;
-    const unsigned nb = ceil_div(3L * b->ntot, 256);
     if (b->precision == SE_FP32)
-        k_factors<float><<<nb, 256, 0, st>>>(b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec,
-                                             b->perm, static_cast<float*>(b->fac), b->PS);
+        k_factors<float><<<ceil_div(3L * b->ntot, factors_threads<float>()),
+                           factors_threads<float>(), 0, st>>>(
+            b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->perm, b->sg,
+            static_cast<float*>(b->fac), b->PS, static_cast<float*>(b->rows));
     else
-        k_factors<double><<<nb, 256, 0, st>>>(b->sys, b->d_part_prefix, b->nsys, b->ntot,
-                                              b->srec, b->perm, static_cast<double*>(b->fac),
-                                              b->PS);
+        k_factors<double><<<ceil_div(3L * b->ntot, factors_threads<double>()),
+                            factors_threads<double>(), 0, st>>>(
+            b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->perm, b->sg,
+            static_cast<double*>(b->fac), b->PS, static_cast<double*>(b->rows));
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     return SE_OK;
@@ -683,11 +760,13 @@ static int run_interp(se_batch b, const double* grid, double* out, double* phi, 
     if (b->precision == SE_FP32)
         k_interp_global<float><<<nb, INTERP_WARPS * 32, 0, st>>>(
             b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->sg, b->perm,
-            static_cast<const float*>(b->fac), b->PS, grid, out, phi);
+            static_cast<const float*>(b->fac), b->PS, static_cast<const float*>(b->rows), grid,
+            out, phi);
     else
         k_interp_global<double><<<nb, INTERP_WARPS * 32, 0, st>>>(
             b->sys, b->d_part_prefix, b->nsys, b->ntot, b->srec, b->sg, b->perm,
-            static_cast<const double*>(b->fac), b->PS, grid, out, phi);
+            static_cast<const double*>(b->fac), b->PS, static_cast<const double*>(b->rows), grid,
+            out, phi);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     return SE_OK;

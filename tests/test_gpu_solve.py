@@ -153,6 +153,34 @@ def test_spread_grid_equals_oracle_wrap(S):
         assert rel(phi, phi_o) < FP64_TOL, (M, P)
 
 
+@pytest.mark.parametrize("M,P,N,clusters", [(32, 16, 3000, 0), (32, 1, 500, 0), (48, 5, 2000, 0),
+                                             (64, 12, 20000, 4), (32, 9, 4000, 2),
+                                             (64, 16, 30000, 0)])
+def test_spread_tile_aligned_rows_equal_oracle(S, M, P, N, clusters):
+    """Grids cut into whole 16^3 tiles with P <= 16 take the tile-aligned
+    spread: every P, tiles at the periodic seam (M = 32: two tiles per axis),
+    crowded clusters; FP64 within 1e-12 of the oracle's grid + wrap, FP32
+    within the FP32 bound of the FP64 grid."""
+    import oracle as O
+    x, q = O.synthetic_system(N, 1.0, seed=M * P + N, charges="uniform", clusters=clusters,
+                              sigma=0.03)
+    m = 0.9 * np.sqrt(O.PI * P)
+    s = O.Setup(M=M, P=P, L=1.0, xi=6.0, m=m, N=N)
+    p = s.params()
+    Hper = O.wrap(p, O.grid_split(p, q, O.base_gaussian(p), O.expand_all(p, x, 3, False)), 3)
+    ref = Hper.reshape(M, M, M).transpose(2, 1, 0)
+    se = S.SpectralEwald(M, P, 1.0, 6.0, m, "potential", "fp64", N)
+    g64 = host(se.spread(cuda(x), cuda(q)))
+    assert rel(g64, ref) < FP64_TOL, rel(g64, ref)
+    s32 = S.SpectralEwald(M, P, 1.0, 6.0, m, "potential", "fp32", N)
+    g32 = host(s32.spread(cuda(x), cuda(q)))
+    assert rel(g32, g64) < 5e-7, rel(g32, g64)
+    # deterministic: a second spread is bit-identical
+    np.testing.assert_array_equal(host(s32.spread(cuda(x), cuda(q))), g32)
+    se.close()
+    s32.close()
+
+
 def test_fp32_spread_grid(S):
     import oracle as O
     M, P, N = 64, 12, 20000
