@@ -69,30 +69,16 @@ __device__ __forceinline__ void set_factors(InterpWarpSmem<T>& W, const SysDev& 
     __syncwarp();
 }
 
-// Where factor 0 of axis a of sorted particle q lives: the tile-aligned row
-// (k_spread2 systems: offset g_a mod 16) or the P-wide row.
-template <typename T>
-__device__ __forceinline__ const T* factor_row(const T* __restrict__ fac, int PS,
-                                               const T* __restrict__ rows, bool aligned,
-                                               long long q, int pk, int a)
-{
-    return aligned ? rows + (q * 3 + a) * 32 + ((pk >> (10 * a)) & 15)
-                   : fac + (q * 3 + a) * PS;
-}
-
-// The same from the factor arrays (lanes < P load their own entries).
+// The same from the factor array (lanes < P load their own entries).
 template <typename T>
 __device__ __forceinline__ void load_factors(InterpWarpSmem<T>& W, const SysDev& S,
-                                             const T* __restrict__ fac, int PS,
-                                             const T* __restrict__ rows, long long p, int pk,
+                                             const T* __restrict__ fac, int PS, long long p,
                                              const double4& rc, int P, int lane)
 {
-    const bool aligned = rows && spread2_eligible(S.M, S.P);
+    const T* f = fac + p * 3 * PS;
     const bool in = lane < P;
-    set_factors(W, S, rc, P, lane,
-                in ? factor_row(fac, PS, rows, aligned, p, pk, 0)[lane] : T(0),
-                in ? factor_row(fac, PS, rows, aligned, p, pk, 1)[lane] : T(0),
-                in ? factor_row(fac, PS, rows, aligned, p, pk, 2)[lane] : T(0));
+    set_factors(W, S, rc, P, lane, in ? f[lane] : T(0), in ? f[PS + lane] : T(0),
+                in ? f[2 * PS + lane] : T(0));
 }
 
 // PT = P at compile time (0: runtime P); plane = pitch between x planes of
@@ -111,6 +97,7 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
     const int beg = boff[bin], end = boff[bin + 1];
     if (beg == end) return;
     const SysDev& S = sys[find_sys(bin_prefix, nsys, bin)];
+    if (rows && spread2_eligible(S.M, S.P)) return;   // k_interp2 covers this system
     const int P = PT ? PT : S.P;
     const int M = S.M;
     const int lb = bin - S.bin_base;
@@ -142,7 +129,6 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
     __syncthreads();
     InterpWarpSmem<T>& W = wsm[warp];
     const bool force = S.mode == SE_FORCE;
-    const bool aligned = rows && spread2_eligible(S.M, S.P);
     // software pipeline: the next particle's record and factors are loaded
     // while the current one is summed
     double4 rc_n = make_double4(0, 0, 0, 0);
@@ -154,9 +140,10 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
             pk_n = sg[q];
             orig_n = sperm[q];
             if (lane < P) {
-                vx_n = factor_row(fac, PS, rows, aligned, q, pk_n, 0)[lane];
-                vy_n = factor_row(fac, PS, rows, aligned, q, pk_n, 1)[lane];
-                vz_n = factor_row(fac, PS, rows, aligned, q, pk_n, 2)[lane];
+                const T* f = fac + (long long)q * 3 * PS;
+                vx_n = f[lane];
+                vy_n = f[PS + lane];
+                vz_n = f[2 * PS + lane];
             }
         }
     };
@@ -257,12 +244,13 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp_global(
     if (p >= ntot) return;
     const int orig = sperm[p];
     const SysDev& S = sys[find_sys(part_prefix, nsys, orig)];
+    if (rows && spread2_eligible(S.M, S.P)) return;   // k_interp2 covers this system
     const int P = S.P, M = S.M;
     InterpWarpSmem<T>& W = wsm[warp];
     const double4 rc = srec[p];
     const int pk = sg[p];
     const int g0 = g_of(pk, 0), g1 = g_of(pk, 1), g2 = g_of(pk, 2);
-    load_factors(W, S, fac, PS, rows, p, pk, rc, P, lane);
+    load_factors(W, S, fac, PS, p, rc, P, lane);
     const bool force = S.mode == SE_FORCE;
     const double* gs = grid + S.grid_off;
     double a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;

@@ -1,0 +1,229 @@
+// se_interp2.cuh -- interpolation (SE_FGG_int / SE_FGG_int_force,
+// SE_fgg.c:968-1100) with the periodic unfold (SE_FGG_extend_fcn,
+// SE_fgg.c:417-443) fused, for the systems k_spread2 serves (whole 16^3
+// tiles, P <= 16).  Included inside namespace se by se_solve.cu after
+// se_interp.cuh.
+//
+// One CTA per fine bin (8^3 stencil corners).  The bin's window, E = 7 + P
+// cells per axis in x and y and EZ = 8 + P rounded up to 4 in z, is copied
+// from the grid (a FP32 copy of it on the FP32 path) with 16-byte loads: the
+// window starts on a multiple of 8 in every axis and M is a multiple of 16,
+// so every 4-cell group is contiguous even where the window wraps.  One warp
+// per particle; lane l takes the (x, y) columns l, l + 32, ... and sums each
+// column over z in pairs: one 8-byte (FP32) or 16-byte (FP64) shared load of
+// two neighbouring cells feeds two packed FMAs per accumulator against the
+// particle's z weights, which are zero-padded pairs in registers aligned to
+// the window.  Columns combine with the x (and y) weights in the working
+// precision; the lanes' sums are reduced in FP64 with shuffles.
+//
+// Shared-memory pitches (row Ep, plane PL) come from the host, chosen so that
+// the pair loads of one instruction fall in distinct banks.
+
+constexpr int I2_WARPS = 8;
+
+template <typename T>
+struct Interp2Warp {
+    T wx[16], fx[16], wy[16], fy[16];   // x, y weights and force weights (-c u)
+    __align__(16) T wz[32];             // z weights shifted to window index
+    __align__(16) T fz[32];
+};
+
+// Two neighbouring window cells and the matching weights.
+template <typename T>
+struct Pair;
+
+template <>
+struct Pair<float> {
+    using V = unsigned long long;
+    __device__ __forceinline__ static V load(const float* p)
+    {
+        return *reinterpret_cast<const V*>(p);
+    }
+    __device__ __forceinline__ static V fma(V a, V b, V c) { return ffma2(a, b, c); }
+    __device__ __forceinline__ static float sum(V v)
+    {
+        const float2 f = f32x2_unpack(v);
+        return f.x + f.y;
+    }
+    __device__ __forceinline__ static V zero() { return 0ull; }
+};
+
+template <>
+struct Pair<double> {
+    using V = double2;
+    __device__ __forceinline__ static V load(const double* p)
+    {
+        return *reinterpret_cast<const double2*>(p);
+    }
+    __device__ __forceinline__ static V fma(V a, V b, V c)
+    {
+        return make_double2(::fma(a.x, b.x, c.x), ::fma(a.y, b.y, c.y));
+    }
+    __device__ __forceinline__ static double sum(V v) { return v.x + v.y; }
+    __device__ __forceinline__ static V zero() { return make_double2(0.0, 0.0); }
+};
+
+// z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
+__host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
+
+template <typename T, int PT>
+__global__ void __launch_bounds__(I2_WARPS * 32) k_interp2(
+    const SysDev* __restrict__ sys, const int* __restrict__ bin_prefix, int nsys,
+    const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ sperm, const T* __restrict__ rows, const int* __restrict__ boff,
+    const T* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out,
+    int Ep, int PL)
+{
+    using PV = Pair<T>;
+    using VT = typename PV::V;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ Interp2Warp<T> wsm[I2_WARPS];
+    const int bin = blockIdx.x;
+    const int beg = boff[bin], end = boff[bin + 1];
+    if (beg == end) return;
+    const SysDev& S = sys[find_sys(bin_prefix, nsys, bin)];
+    if (!spread2_eligible(S.M, S.P)) return;   // k_interp covers this system
+    const int P = PT ? PT : S.P;
+    const int M = S.M;
+    const int lb = bin - S.bin_base;
+    const int o0 = (lb / (S.nf[1] * S.nf[2])) * FB;
+    const int o1 = ((lb / S.nf[2]) % S.nf[1]) * FB;
+    const int o2 = (lb % S.nf[2]) * FB;
+    const int E = FB + P - 1, EZ = interp2_ez(P);
+    T* tile = reinterpret_cast<T*>(dsm);
+    const T* gs = grid + S.grid_off;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    // ---- stage the window: rows (a, b), groups of 4 cells along z
+    {
+        constexpr int G = 4;
+        const int ng = EZ / G;
+        for (int u = threadIdx.x; u < E * E * ng; u += blockDim.x) {
+            const int row = u / ng, g = u - row * ng;
+            const int a = row / E, b = row - a * E;
+            int x = o0 + a, y = o1 + b, z = o2 + g * G;
+            x -= x >= M ? M : 0;
+            y -= y >= M ? M : 0;
+            z -= z >= M ? M : 0;
+            const T* src = gs + ((long long)x * M + y) * M + z;
+            T* dst = tile + a * PL + b * Ep + g * G;
+            if constexpr (sizeof(T) == 4) {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(src));
+                reinterpret_cast<float2*>(dst)[0] = make_float2(v.x, v.y);
+                reinterpret_cast<float2*>(dst)[1] = make_float2(v.z, v.w);
+            } else {
+                const double2 v0 = __ldg(reinterpret_cast<const double2*>(src));
+                const double2 v1 = __ldg(reinterpret_cast<const double2*>(src) + 1);
+                reinterpret_cast<double2*>(dst)[0] = v0;
+                reinterpret_cast<double2*>(dst)[1] = v1;
+            }
+        }
+    }
+    __syncthreads();
+
+    Interp2Warp<T>& W = wsm[warp];
+    const bool force = S.mode == SE_FORCE;
+    constexpr int NQ = PT ? PT / 2 + 1 : 9;   // z pairs a stencil spans (<= 9 for P <= 16)
+    const int nq = P / 2 + 1;
+    const bool JFIX = (32 % P) == 0;
+    for (int p = beg + warp; p < end; p += I2_WARPS) {
+        const double4 rc = srec[p];
+        const int pk = sg[p];
+        const int orig = sperm[p];
+        const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
+        const int r0 = gx - o0, r1 = gy - o1, r2 = gz - o2;
+        // weights: lane i < P holds factor i of each axis (tile-aligned rows)
+        const T* rb = rows + (long long)p * 96;
+        W.wz[lane] = T(0);
+        W.fz[lane] = T(0);
+        __syncwarp();
+        if (lane < P) {
+            const double off = (S.lo + lane) * S.h;
+            const T vx = rb[(gx & 15) + lane], vy = rb[32 + (gy & 15) + lane],
+                    vz = rb[64 + (gz & 15) + lane];
+            W.wx[lane] = vx;
+            W.wy[lane] = vy;
+            W.wz[r2 + lane] = vz;
+            if (force) {
+                W.fx[lane] = (T)((double)vx * (-S.c * (rc.x - off)));
+                W.fy[lane] = (T)((double)vy * (-S.c * (rc.y - off)));
+                W.fz[r2 + lane] = (T)((double)vz * (-S.c * (rc.z - off)));
+            }
+        }
+        __syncwarp();
+        const int q0 = r2 >> 1;
+        VT wz2[NQ], fz2[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            if (PT || q < nq) {
+                wz2[q] = PV::load(W.wz + 2 * (q0 + q));
+                fz2[q] = force ? PV::load(W.fz + 2 * (q0 + q)) : PV::zero();
+            }
+        }
+        T a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
+        for (int c = lane; c < P * P; c += 32) {
+            const int i = c / P, j = c - (c / P) * P;
+            const T* col = tile + (r0 + i) * PL + (r1 + j) * Ep + 2 * q0;
+            VT s0 = PV::zero(), s1 = PV::zero();
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                if (PT || q < nq) {
+                    const VT g2 = PV::load(col + 2 * q);
+                    s0 = PV::fma(g2, wz2[q], s0);
+                    if (force) s1 = PV::fma(g2, fz2[q], s1);
+                }
+            }
+            const T t0 = PV::sum(s0);
+            const T wxi = W.wx[i];
+            if (JFIX) {   // j is the lane's own: the y weights multiply once below
+                a_pot = fma(t0, wxi, a_pot);
+                if (force) {
+                    a_fx = fma(t0, W.fx[i], a_fx);
+                    a_fz = fma(PV::sum(s1), wxi, a_fz);
+                }
+            } else {
+                const T wyj = W.wy[j];
+                const T wij = wxi * wyj;
+                a_pot = fma(t0, wij, a_pot);
+                if (force) {
+                    a_fx = fma(t0, W.fx[i] * wyj, a_fx);
+                    a_fy = fma(t0, wxi * W.fy[j], a_fy);
+                    a_fz = fma(PV::sum(s1), wij, a_fz);
+                }
+            }
+        }
+        double d_pot = a_pot, d_fx = a_fx, d_fy = a_fy, d_fz = a_fz;
+        if (JFIX) {
+            const int j = lane % P;
+            const double wyj = (double)W.wy[j];
+            if (force) {
+                d_fy = d_pot * (double)W.fy[j];
+                d_fx *= wyj;
+                d_fz *= wyj;
+            }
+            d_pot *= wyj;
+        }
+        d_pot = warp_sum(d_pot);
+        if (force) {
+            d_fx = warp_sum(d_fx);
+            d_fy = warp_sum(d_fy);
+            d_fz = warp_sum(d_fz);
+        }
+        if (lane == 0)
+            interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz, force, out,
+                         phi_out);
+        __syncwarp();
+    }
+}
+
+// Every FP64 grid value of the batch as FP32 (the staged source of
+// k_interp2<float>), two values per thread step.
+__global__ void k_grid_to_f32(const double2* __restrict__ in, float2* __restrict__ out,
+                              long long n2)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n2;
+         e += (long long)gridDim.x * blockDim.x) {
+        const double2 v = in[e];
+        out[e] = make_float2((float)v.x, (float)v.y);
+    }
+}

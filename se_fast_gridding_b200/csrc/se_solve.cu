@@ -210,6 +210,7 @@ __global__ void k_scale(const SysDev* __restrict__ sys, double2* __restrict__ sp
 }
 
 #include "se_interp.cuh"
+#include "se_interp2.cuh"
 
 // ---------------------------------------------------------------- energy --
 
@@ -283,6 +284,11 @@ struct se_batch_s {
     int PS = 0;
     void* rows = nullptr;     // tile-aligned rows [ntot][3][32] (k_spread2 systems)
     bool any_spread1 = false, any_spread2 = false;
+    float* grid32 = nullptr;  // FP32 copy of the grids, staged by k_interp2<float>
+    int i2_P = 0;             // largest P of the k_interp2 systems (0: none)
+    bool i2_uniform = false;  // all k_interp2 systems have P == i2_P
+    int i2_Ep = 0, i2_PL = 0; // k_interp2 window pitches
+    size_t i2_smem = 0;
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     double* grid = nullptr;
@@ -392,7 +398,7 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
         ntot += sys[i].N;
         nbins += (long long)nf * nf * nf;
         ntiles += (long long)((M + TX - 1) / TX) * ((M + TY - 1) / TY) * ((M + TZ - 1) / TZ);
-        grid += (long long)M * M * M;
+        grid += (long long)M * M * M + 16;
         spec += (long long)M * M * (M / 2 + 1);
     }
     if (nbins_out) *nbins_out = (int)nbins;
@@ -408,6 +414,7 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     }
     if (plain) b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
     if (rows) b += (size_t)ntot * 3 * 32 * (precision == SE_FP32 ? 4 : 8);
+    if (rows && precision == SE_FP32) b += (size_t)grid * 4;   // FP32 copy of the grids
     b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
     b += (size_t)(nbins + 1) * 4;
     b += (size_t)grid * 8 + (size_t)spec * 16;
@@ -428,7 +435,8 @@ static int batch_free(se_batch b)
         if (e) cudaEventDestroy(e);
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
-                    b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows};
+                    b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows,
+                    b->grid32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -481,6 +489,52 @@ static cudaError_t raise_smem_limit(const void* fn, size_t smem)
     return e;
 }
 
+// Row pitch Ep and plane pitch PL (elements, both even) of k_interp2's
+// window for stencils up to P: the pair loads of one warp instruction (lane
+// l reads column c = l + 32 m, i = c / P, j = c % P) are served in 128-byte
+// groups of lanes; count, over all rounds m, the largest number of distinct
+// 4-byte words that share a bank within a group, and keep the smallest.
+static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
+{
+    const int E = FB + P - 1, EZ = interp2_ez(P);
+    const int words = precision == SE_FP32 ? 2 : 4;   // 4-byte words per pair
+    const int group = 32 / words;                     // lanes per 128 bytes
+    int best_cost = 1 << 30, best_Ep = EZ, best_PL = E * EZ;
+    for (int Ep = EZ; Ep <= EZ + 32; Ep += 2) {
+        for (int pad = 0; pad <= 64; pad += 2) {
+            const int PL = E * Ep + pad;
+            int cost = 0;
+            for (int m = 0; m * 32 < P * P; m++) {
+                for (int g0 = 0; g0 < 32; g0 += group) {
+                    int wordsat[32][8];
+                    int nw[32] = {0};
+                    int worst = 0;
+                    for (int l = g0; l < g0 + group; l++) {
+                        const int c = l + 32 * m;
+                        if (c >= P * P) continue;
+                        const int e = (c / P) * PL + (c % P) * Ep;   // element offset
+                        for (int w = 0; w < words; w++) {
+                            const int word = e * (words / 2) + w, bank = word & 31;
+                            bool seen = false;
+                            for (int k = 0; k < nw[bank]; k++) seen = seen || wordsat[bank][k] == word;
+                            if (!seen && nw[bank] < 8) wordsat[bank][nw[bank]++] = word;
+                            worst = std::max(worst, nw[bank]);
+                        }
+                    }
+                    cost += worst;
+                }
+            }
+            if (cost < best_cost) {
+                best_cost = cost;
+                best_Ep = Ep;
+                best_PL = PL;
+            }
+        }
+    }
+    *Ep_out = best_Ep;
+    *PL_out = best_PL;
+}
+
 static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision)
 {
     if (!out || !systems || nsys < 1 || (precision != SE_FP64 && precision != SE_FP32))
@@ -501,6 +555,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         const int i = order[k];
         const int M = systems[i].M;
         if (b->groups.empty() || b->groups.back().M != M) {
+            gcur = (gcur + 15) & ~15LL;   // every group's grids start 128-byte aligned
             FftGroup g{};
             g.M = M;
             g.count = 0;
@@ -580,6 +635,18 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     }
     if (b->any_spread1) SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
     if (b->any_spread2) SE_ALLOC(b->rows, nt * 3 * 32 * (precision == SE_FP32 ? 4 : 8));
+    if (b->any_spread2 && precision == SE_FP32)
+        SE_ALLOC(b->grid32, sizeof(float) * b->grid_elems);
+    if (b->any_spread2) {
+        b->i2_uniform = true;
+        for (int i = 0; i < nsys; i++) {
+            if (!spread2_eligible(systems[i].M, systems[i].P)) continue;
+            if (b->i2_P && systems[i].P != b->i2_P) b->i2_uniform = false;
+            b->i2_P = std::max(b->i2_P, systems[i].P);
+        }
+        interp2_pitch(b->i2_P, precision, &b->i2_Ep, &b->i2_PL);
+        b->i2_smem = (size_t)(FB + b->i2_P - 1) * b->i2_PL * (precision == SE_FP32 ? 4 : 8);
+    }
     b->sort_bytes = sort_scratch_bytes(b->ntot, std::max(b->nbins, 1));
     SE_ALLOC(b->sort_scratch, b->sort_bytes);
     SE_ALLOC(b->grid, sizeof(double) * b->grid_elems);
@@ -749,9 +816,49 @@ static int run_factors(se_batch b, cudaStream_t st)
     return SE_OK;
 }
 
+template <typename T>
+static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, cudaStream_t st)
+{
+    const int P = b->i2_P;
+    const bool u = b->i2_uniform;
+    const void* fn = (u && P == 8)    ? (const void*)k_interp2<T, 8>
+                     : (u && P == 12) ? (const void*)k_interp2<T, 12>
+                     : (u && P == 16) ? (const void*)k_interp2<T, 16>
+                                      : (const void*)k_interp2<T, 0>;
+    SE_CUDA(raise_smem_limit(fn, b->i2_smem));
+    const dim3 grd(std::max(b->nbins, 1)), blk(I2_WARPS * 32);
+    const T* rows = static_cast<const T*>(b->rows);
+#define SE_I2ARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, rows, b->boff, grid, \
+                  out, phi, b->i2_Ep, b->i2_PL
+    if (u && P == 8) k_interp2<T, 8><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    else if (u && P == 12) k_interp2<T, 12><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    else if (u && P == 16) k_interp2<T, 16><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    else k_interp2<T, 0><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+#undef SE_I2ARGS
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
 static int run_interp(se_batch b, const double* grid, double* out, double* phi, cudaStream_t st)
 {
     if (b->ntot == 0) return SE_OK;
+    // systems of whole 16^3 tiles with P <= 16: k_interp2 (FP32 path from an
+    // FP32 copy of the grids); the others: k_interp / k_interp_global
+    if (b->any_spread2) {
+        if (b->precision == SE_FP32) {
+            const long long n = b->grid_elems;
+            k_grid_to_f32<<<std::min<long long>(4096, ceil_div(n / 2 + 1, 256)), 256, 0, st>>>(
+                reinterpret_cast<const double2*>(grid), reinterpret_cast<float2*>(b->grid32),
+                n / 2);
+            SE_CUDA(cudaGetLastError());
+            LAUNCHED(b);
+            SE_TRY(launch_interp2<float>(b, b->grid32, out, phi, st));
+        } else {
+            SE_TRY(launch_interp2<double>(b, grid, out, phi, st));
+        }
+    }
+    if (!b->any_spread1) return SE_OK;
     if (b->staged_interp) {
         if (b->precision == SE_FP32) return launch_interp_staged<float>(b, grid, out, phi, st);
         return launch_interp_staged<double>(b, grid, out, phi, st);
@@ -993,7 +1100,14 @@ extern "C" int se_spread(se_plan p, int N, const double* x, const double* q, dou
     p->b->launches = p->b->pending_launches;
     p->b->pending_launches = 0;
     SE_TRY(run_prepare_sort(p->b, x, q, st));
-    return run_spread(p->b, grid, st);
+    // the tile kernels store 16-byte pairs: a caller grid that is not
+    // 16-byte aligned is filled through the plan's own grid
+    if (reinterpret_cast<uintptr_t>(grid) % 16 == 0) return run_spread(p->b, grid, st);
+    SE_TRY(run_spread(p->b, p->b->grid, st));
+    const long long M = p->cfg.M;
+    SE_CUDA(cudaMemcpyAsync(grid, p->b->grid, sizeof(double) * M * M * M,
+                            cudaMemcpyDeviceToDevice, st));
+    return SE_OK;
 }
 
 extern "C" int se_kspace(se_plan p, double* grid, void* stream)
@@ -1011,6 +1125,14 @@ extern "C" int se_interp(se_plan p, int N, const double* x, const double* q, con
     p->b->launches = p->b->pending_launches;
     p->b->pending_launches = 0;
     SE_TRY(run_prepare_sort(p->b, x, q, st));
+    // the window kernels read 16-byte groups: a caller grid that is not
+    // 16-byte aligned is read through the plan's own grid
+    if (reinterpret_cast<uintptr_t>(grid) % 16 != 0) {
+        const long long M = p->cfg.M;
+        SE_CUDA(cudaMemcpyAsync(p->b->grid, grid, sizeof(double) * M * M * M,
+                                cudaMemcpyDeviceToDevice, st));
+        grid = p->b->grid;
+    }
     return run_interp(p->b, grid, out, phi_out, st);
 }
 

@@ -177,8 +177,34 @@ def test_spread_tile_aligned_rows_equal_oracle(S, M, P, N, clusters):
     assert rel(g32, g64) < 5e-7, rel(g32, g64)
     # deterministic: a second spread is bit-identical
     np.testing.assert_array_equal(host(s32.spread(cuda(x), cuda(q))), g32)
+    # interpolation of a given grid = extend + int_split (window pair sums)
+    rng = np.random.Generator(np.random.Philox(M + P))
+    field = rng.standard_normal((M, M, M))
+    Hp = np.ascontiguousarray(field.transpose(2, 1, 0)).reshape(-1)
+    phi_o = O.int_split(p, O.extend(p, Hp, 3), O.base_gaussian(p), O.expand_all(p, x, 3, False))
+    phi64 = host(se.interp(cuda(x), cuda(q), cuda(field)))
+    assert rel(phi64, phi_o) < FP64_TOL, rel(phi64, phi_o)
+    phi32 = host(s32.interp(cuda(x), cuda(q), cuda(field)))
+    assert rel(phi32, phi_o) < 1e-6, rel(phi32, phi_o)
+    # caller grids that are not 16-byte aligned give the same numbers
+    import torch
+    buf = torch.zeros(M ** 3 + 1, dtype=torch.float64, device="cuda")
+    np.testing.assert_array_equal(host(se.spread(cuda(x), cuda(q), grid=buf[1:])),
+                                  g64.reshape(-1))
+    buf[1:] = cuda(field).reshape(-1)
+    np.testing.assert_array_equal(host(se.interp(cuda(x), cuda(q), buf[1:])), phi64)
+    np.testing.assert_array_equal(host(s32.interp(cuda(x), cuda(q), buf[1:])), phi32)
     se.close()
     s32.close()
+    # full FORCE solve against the oracle pipeline
+    f = S.SpectralEwald(M, P, 1.0, 6.0, m, "force", "fp64", N)
+    got = host(f.solve(cuda(x), cuda(q)))
+    ref = O.spectral_ewald(x, q, M, P, m, 1.0, 6.0, "force")
+    assert rel(got, ref) < FP64_TOL, rel(got, ref)
+    f32 = S.SpectralEwald(M, P, 1.0, 6.0, m, "force", "fp32", N)
+    assert rel(host(f32.solve(cuda(x), cuda(q))), ref) < 1e-6
+    f.close()
+    f32.close()
 
 
 def test_fp32_spread_grid(S):
