@@ -187,17 +187,24 @@ __device__ __forceinline__ double kwave(int i, int M, double kfac)
 
 // spec *= Z on the half spectrum [x][y][z <= M/2]; Z = exp(scalar K2)/K2 * 4pi/M^3
 // with K2 summed in the reference's order (its first FFT axis is our z).
-__global__ void k_scale(const SysDev* __restrict__ sys, double2* __restrict__ spec)
+constexpr int SCALE_THREADS = 256, SCALE_ITEMS = 8;
+
+// Elements e = blockIdx.x * SCALE_THREADS * SCALE_ITEMS + ... of one
+// system's half spectrum [x][y][z <= M/2]; 32-bit index arithmetic.
+__global__ void __launch_bounds__(SCALE_THREADS) k_scale(const SysDev* __restrict__ sys,
+                                                         double2* __restrict__ spec)
 {
     const SysDev& S = sys[blockIdx.y];
     const int M = S.M, Mh = M / 2 + 1;
-    const long long n = (long long)M * M * Mh;
+    const int n = M * M * Mh;
     double2* sp = spec + S.spec_off;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int iz = (int)(e % Mh);
-        const int iy = (int)((e / Mh) % M);
-        const int ix = (int)(e / ((long long)Mh * M));
+    const int e0 = blockIdx.x * (SCALE_THREADS * SCALE_ITEMS) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < SCALE_ITEMS; k++) {
+        const int e = e0 + k * SCALE_THREADS;
+        if (e >= n) break;
+        const int r = e / Mh, iz = e - r * Mh;
+        const int ix = r / M, iy = r - ix * M;
         const double kx = kwave(ix, M, S.kfac), ky = kwave(iy, M, S.kfac),
                      kz = kwave(iz, M, S.kfac);
         const double K2 = (kz * kz + ky * ky) + kx * kx;
@@ -762,8 +769,11 @@ static int run_kspace(se_batch b, double* grid, cudaStream_t st)
         SE_CUFFT(cufftExecD2Z(g.fwd, grid + g.grid_off,
                               reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off)));
     }
-    dim3 gs(std::min<long long>(1024, ceil_div(b->spec_elems / b->nsys + 1, 256)), b->nsys);
-    k_scale<<<gs, 256, 0, st>>>(b->sys, b->spec);
+    int maxM = 0;
+    for (auto& g : b->groups) maxM = std::max(maxM, g.M);
+    const dim3 gs(ceil_div((long)maxM * maxM * (maxM / 2 + 1), SCALE_THREADS * SCALE_ITEMS),
+                  b->nsys);
+    k_scale<<<gs, SCALE_THREADS, 0, st>>>(b->sys, b->spec);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     for (auto& g : b->groups) {

@@ -18,6 +18,7 @@ namespace {
 constexpr int SCAN_THREADS = 1024;
 constexpr int SCAN_ITEMS = 4;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+constexpr long SCAN_BLOCK_MAX = 16L * SCAN_TILE;   // scanned by one block
 
 constexpr int RADIX_BITS = 8;
 constexpr int RADIX = 1 << RADIX_BITS;
@@ -74,6 +75,60 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tile(const int* __restric
         if (tile_sums) tile_sums[blockIdx.x] = run;
         if (total_out) *total_out = run;
     }
+}
+
+// Exclusive scan of a short array by one block: tiles of SCAN_TILE in order,
+// each offset by the running total of the ones before (in place allowed).
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_block(const int* in, int* out, long n,
+                                                             int* total_out)
+{
+    __shared__ int wsum[SCAN_THREADS / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int carry = 0;
+    for (long t0 = 0; t0 < n; t0 += SCAN_TILE) {
+        const long idx = t0 + (long)threadIdx.x * SCAN_ITEMS;
+        int v[SCAN_ITEMS];
+        int t = 0;
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; i++) {
+            v[i] = (idx + i < n) ? in[idx + i] : 0;
+            t += v[i];
+        }
+        const int incl = warp_incl_scan(t);
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int s = wsum[lane];
+            const int si = warp_incl_scan(s);
+            wsum[lane] = si;
+        }
+        __syncthreads();
+        int run = carry + incl - t + (warp ? wsum[warp - 1] : 0);
+#pragma unroll
+        for (int i = 0; i < SCAN_ITEMS; i++) {
+            if (idx + i < n) out[idx + i] = run;
+            run += v[i];
+        }
+        carry += wsum[31];
+        __syncthreads();   // wsum reused by the next tile
+    }
+    if (total_out && threadIdx.x == 0) *total_out = carry;
+}
+
+// offsets[k] = the first position of sorted[0, N) holding a key >= k, for
+// k <= nkeys: the start of each key's run (offsets[nkeys] = N).
+__global__ void k_key_bounds(const int* __restrict__ sorted, int N, int nkeys,
+                             int* __restrict__ offsets)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > nkeys) return;
+    int lo = 0, hi = N;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (sorted[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    offsets[k] = lo;
 }
 
 __global__ void k_scan_add(int* out, long n, const int* __restrict__ tile_offs, int ntiles,
@@ -143,12 +198,6 @@ __global__ void __launch_bounds__(SORT_THREADS) k_radix_scatter(
     }
 }
 
-__global__ void k_key_count(const int* __restrict__ keys, int N, int* counts)
-{
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) atomicAdd(&counts[keys[i]], 1);
-}
-
 __global__ void k_iota(int* out, int N)
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -167,7 +216,7 @@ int radix_passes(int nkeys)
 size_t scan_scratch_bytes(long n)
 {
     const long nt = (n + SCAN_TILE - 1) / SCAN_TILE;
-    if (nt <= 1) return 0;
+    if (n <= SCAN_BLOCK_MAX) return 0;
     return align_up(sizeof(int) * (nt + 1)) + scan_scratch_bytes(nt);
 }
 
@@ -179,8 +228,8 @@ int exclusive_scan(const int* in, int* out, long n, bool write_total, void* scra
         return SE_OK;
     }
     const long nt = (n + SCAN_TILE - 1) / SCAN_TILE;
-    if (nt == 1) {
-        k_scan_tile<<<1, SCAN_THREADS, 0, st>>>(in, out, n, nullptr, write_total ? out + n : nullptr);
+    if (n <= SCAN_BLOCK_MAX) {   // one block, one launch
+        k_scan_block<<<1, SCAN_THREADS, 0, st>>>(in, out, n, write_total ? out + n : nullptr);
         SE_CUDA(cudaGetLastError());
         if (launches) (*launches)++;
         return SE_OK;
@@ -205,9 +254,7 @@ size_t sort_scratch_bytes(int N, int nkeys)
     b += 4 * align_up(sizeof(int) * (size_t)(N > 0 ? N : 1));          // keys/vals ping-pong
     b += align_up(sizeof(int) * (size_t)(N > 0 ? N : 1));              // sorted keys if not wanted
     b += align_up(sizeof(int) * (size_t)(hist + 1));
-    b += align_up(sizeof(int) * (size_t)(nkeys + 1));
-    const size_t s1 = scan_scratch_bytes(hist), s2 = scan_scratch_bytes(nkeys);
-    b += align_up(s1 > s2 ? s1 : s2);
+    b += align_up(scan_scratch_bytes(hist));
     return b;
 }
 
@@ -227,20 +274,18 @@ int stable_sort(const int* keys, const int* vals_in, int N, int nkeys, int* perm
     const long ntiles = (N + SORT_TILE - 1) / SORT_TILE;
     const long nhist = (long)RADIX * (ntiles > 0 ? ntiles : 1);
     int* hist = reinterpret_cast<int*>(p); p += align_up(sizeof(int) * (size_t)(nhist + 1));
-    int* counts = reinterpret_cast<int*>(p); p += align_up(sizeof(int) * (size_t)(nkeys + 1));
     void* sscr = p;
     int* kfinal = sorted_keys ? sorted_keys : kS;
 
-    if (offsets) {
-        SE_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nkeys, st));
-        if (N > 0) {
-            k_key_count<<<ceil_div(N, 256), 256, 0, st>>>(keys, N, counts);
-            SE_CUDA(cudaGetLastError());
-            if (launches) (*launches)++;
-        }
-        SE_TRY(exclusive_scan(counts, offsets, nkeys, true, sscr, st, launches));
-    }
-    if (N == 0) return SE_OK;
+    // the start of every key's run, from the sorted keys
+    auto bounds = [&](const int* sorted) -> int {
+        if (!offsets) return SE_OK;
+        k_key_bounds<<<ceil_div((long)nkeys + 1, 256), 256, 0, st>>>(sorted, N, nkeys, offsets);
+        SE_CUDA(cudaGetLastError());
+        if (launches) (*launches)++;
+        return SE_OK;
+    };
+    if (N == 0) return bounds(keys);
     const int passes = radix_passes(nkeys);
     if (passes == 0) {   // a single key: the identity permutation
         k_iota<<<ceil_div(N, 256), 256, 0, st>>>(perm, N);
@@ -248,7 +293,7 @@ int stable_sort(const int* keys, const int* vals_in, int N, int nkeys, int* perm
         if (launches) (*launches)++;
         if (sorted_keys) SE_CUDA(cudaMemcpyAsync(sorted_keys, keys, sizeof(int) * N,
                                                  cudaMemcpyDeviceToDevice, st));
-        return SE_OK;
+        return bounds(keys);
     }
     const int* kin = keys;
     const int* vin = vals_in;
@@ -267,7 +312,7 @@ int stable_sort(const int* keys, const int* vals_in, int N, int nkeys, int* perm
         kin = kout;
         vin = vout;
     }
-    return SE_OK;
+    return bounds(kfinal);
 }
 
 }  // namespace se
