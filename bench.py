@@ -204,14 +204,34 @@ def run_batched(args):
     if pg:
         t = shard.max_over_ranks(t)
     ntot_all = sum(s["N"] for s in allsys)
-    # accuracy of a few systems: FP32 batch vs FP64 single solves
+    # the plain FP64 single-system path on the same inputs: one plan per
+    # system, the systems solved one after another (L2 flushed first); and the
+    # accuracy of the FP32 batch against it
     errs = []
     outs = b.split(out)
-    for j in range(min(4, len(systems))):
-        s = systems[j]
-        se = solver.SpectralEwald(s.M, s.P, s.L, s.xi, None, "potential", "fp64", s.N)
-        ref = se.solve(torch.tensor(xs[j], device=dev), torch.tensor(qs[j], device=dev))
-        errs.append(O.rel_rms(outs[j].cpu().numpy(), ref.cpu().numpy()))
+    plans = [solver.SpectralEwald(s.M, s.P, s.L, s.xi, None, "potential", "fp64", s.N)
+             for s in systems]
+    xd = [torch.tensor(v, device=dev) for v in xs]
+    qd = [torch.tensor(v, device=dev) for v in qs]
+    od = [torch.empty(s.N, dtype=torch.float64, device=dev) for s in systems]
+    for se, a, c, o in zip(plans, xd, qd, od):
+        se.solve(a, c, o)
+    t64 = []
+    for k in range(3):
+        flush.fill_(float(k))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for se, a, c, o in zip(plans, xd, qd, od):
+            se.solve(a, c, o)
+        e1.record(stream)
+        e1.synchronize()
+        t64.append(e0.elapsed_time(e1))
+    fp64_ms = sum(t64) / len(t64)
+    if pg:
+        fp64_ms = shard.max_over_ranks(fp64_ms)
+    for j in range(len(systems)):
+        errs.append(O.rel_rms(outs[j].cpu().numpy(), od[j].cpu().numpy()))
+    for se in plans:
         se.close()
     if rank == 0:
         line = {
@@ -225,7 +245,11 @@ def run_batched(args):
                        "systems": 256, "particles": ntot_all,
                        "l2": "flushed between steps (256 MiB write)"},
             "solves_per_s": 256 / (t * 1e-3), "stage_ms": {k: sum(v) / len(v) for k, v in stage.items()},
-            "gpu_launches": launches, "accuracy": {"rel_rms_fp32_vs_fp64_4_systems": max(errs)},
+            "gpu_launches": launches,
+            "accuracy": {"rel_rms_fp32_vs_fp64_max_over_systems": max(errs)},
+            "fp64_plain": {"ms_per_step": fp64_ms, "fp32_batched_speedup": fp64_ms / t,
+                           "note": "the same systems solved one by one on FP64 single-system "
+                                   "plans (3 steps, L2 flushed)"},
         }
         print(json.dumps(line), flush=True)
     b.close()
@@ -287,9 +311,10 @@ def run_large(args):
 def run_serve(args):
     """C4: Poisson arrivals of POTENTIAL/FORCE solves (50/50), N log-uniform in
     [500, 2e6], P in {8, 12, 16}, through the native request loop (8 slots,
-    120 GB budget), host (pinned) inputs and outputs.  Each trace is replayed
-    once untimed (plan and pinned-buffer caches warm) and once timed; latency
-    is submit to result-in-host-memory on the host clock."""
+    120 GB budget), host (pinned) inputs and outputs; the results go to one
+    pinned buffer made before any replay.  Each trace is replayed once untimed
+    (plan cache warm) and once timed; latency is submit to result-in-host-
+    memory on the host clock."""
     import torch
     from se_fast_gridding_b200 import serve
     rank, world, local = dist_env()
@@ -297,19 +322,23 @@ def run_serve(args):
     xs, qs = serve.particle_pool()
     rates = [2000.0] if args.serve_rates is None else [float(r) for r in args.serve_rates.split(",")]
     runs = []
+    traces = [(literal, rate, serve.poisson_trace(rate, args.serve_seconds, seed=4 + rank,
+                                                  literal_grid=literal))
+              for literal in (False, True) for rate in rates]
+    # pinned result buffers for the largest trace, made before any replay
+    arena = serve.output_arena(max((t for _, _, t in traces),
+                                   key=lambda tr: sum(r.system.out_width * r.system.N
+                                                      for r in tr)))
     with serve.Server(slots=args.serve_slots, precision="fp32", hbm_budget=120 * 10 ** 9) as srv:
-        for literal in (False, True):
-            for rate in rates:
-                trace = serve.poisson_trace(rate, args.serve_seconds, seed=4 + rank,
-                                            literal_grid=literal)
-                serve.replay(srv, trace, xs, qs)                       # warm
-                comps, _, wall, lag = serve.replay(srv, trace, xs, qs)  # timed
-                parts = sum(r.system.N for r in trace)
-                lat = serve.latency_summary(comps)
-                runs.append({"grid": "M=64 for all" if literal else "M=64*2^ceil(log2(N/16000)/3) <= 256",
-                             "offered_req_s": rate, "requests": len(trace),
-                             "solves_per_s": len(comps) / wall, "particles_per_s": parts / wall,
-                             "wall_s": wall, "max_submit_lag_ms": lag * 1e3, **lat})
+        for literal, rate, trace in traces:
+            serve.replay(srv, trace, xs, qs, arena)                       # warm
+            comps, _, wall, lag = serve.replay(srv, trace, xs, qs, arena)  # timed
+            parts = sum(r.system.N for r in trace)
+            lat = serve.latency_summary(comps)
+            runs.append({"grid": "M=64 for all" if literal else "M=64*2^ceil(log2(N/16000)/3) <= 256",
+                         "offered_req_s": rate, "requests": len(trace),
+                         "solves_per_s": len(comps) / wall, "particles_per_s": parts / wall,
+                         "wall_s": wall, "max_submit_lag_ms": lag * 1e3, **lat})
         st = srv.stats()
     head = runs[rates.index(2000.0) if 2000.0 in rates else 0]
     if rank == 0:
@@ -408,11 +437,29 @@ def main():
     # accuracy (rank 0, outside the timed region): FP32 vs the FP64 path and
     # vs the FP64 direct k-space sum on the 1,000-particle subset
     accuracy = None
+    fp64_ms = None
     if rank == 0:
         se.solve(x, q, out)
         f32 = out.cpu().numpy()
         s64 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp64", N)
         f64 = s64.solve(x, q).cpu().numpy()
+        # the plain FP64 path on the same inputs, timed the same way (the
+        # FP32 path is measured against it)
+        fl = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+        o64 = torch.empty(3 * N, dtype=torch.float64, device=dev)
+        for _ in range(3):
+            s64.solve(x, q, o64)
+        t64 = []
+        for k in range(5):
+            fl.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s64.solve(x, q, o64)
+            b.record(stream)
+            b.synchronize()
+            t64.append(a.elapsed_time(b))
+        fp64_ms = sum(t64) / len(t64)
+        del fl, o64
         s64.close()
         accuracy = {"rel_rms_fp32_vs_fp64": O.rel_rms(f32, f64)}
         gpath = os.path.join(ROOT, "tests", "golden", "c2.npz")
@@ -506,12 +553,13 @@ def main():
     traffic = None
     if tr and tr.get("workload") == workload_name(w):
         traffic = tr.get(dom)
-    roofline = {"kernel": f"k_{dom}", "bound": "hbm", "achieved": alg_bytes / t_dom / 1e9,
+    kname = f"k_{dom}2" if (M % 16 == 0 and M >= 32 and P <= 16) else f"k_{dom}"
+    roofline = {"kernel": kname, "bound": "hbm", "achieved": alg_bytes / t_dom / 1e9,
                 "peak": hbm, "unit": "GB/s", "frac": alg_bytes / t_dom / 1e9 / hbm,
                 "traffic": traffic, "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if hbm_kind == "measured" else "fallback 6650 GB/s",
                 "algorithmic_bytes": alg_bytes}
-    roofline_fma = {"kernel": f"k_{dom}", "bound": "fp32_fma", "achieved": flops / t_dom / 1e12,
+    roofline_fma = {"kernel": kname, "bound": "fp32_fma", "achieved": flops / t_dom / 1e12,
                     "peak": fma, "unit": "TFLOP/s", "frac": flops / t_dom / 1e12 / fma,
                     "peak_source": "measured FMA-chain kernel (se_probe_fma_tflops)"}
     cpu = None
@@ -538,6 +586,9 @@ def main():
                 "ms_per_step": e2e},
         "gpu_launches": launches,
         "clocks": clk, "accuracy": accuracy, "wall_s_timed": wall,
+        "fp64_plain": None if fp64_ms is None else {
+            "ms_per_step": fp64_ms, "fp32_speedup": fp64_ms / ms,
+            "note": "the FP64 path on the same inputs, same timing (5 steps, L2 flushed)"},
     }
     print(json.dumps(line), flush=True)
     se.close()

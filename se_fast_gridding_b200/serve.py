@@ -182,14 +182,26 @@ def particle_pool(size: int = 6_000_000, L: float = 1.0, seed: int = 7, pin: boo
     return xs, qs
 
 
+def output_arena(trace: list[TraceRequest], pin: bool = True) -> torch.Tensor:
+    """One host buffer holding every request's output of a trace back to back
+    (pinned: allocating pinned memory while the GPU is busy can wait for it
+    to go idle, so a server's result buffers are set up beforehand)."""
+    n = sum(r.system.out_width * r.system.N for r in trace)
+    return torch.empty(max(n, 1), dtype=torch.float64, pin_memory=pin)
+
+
 def replay(server: Server, trace: list[TraceRequest], xs: torch.Tensor, qs: torch.Tensor,
-           keep_outputs: bool = False):
+           arena: torch.Tensor | None = None, keep_outputs: bool = False):
     """Submit each request at its arrival time (real time), collect the
-    completions.  Returns (completions by ticket, outputs by ticket or None,
-    wall seconds from the first arrival to the last completion, the largest
-    lag of a submission behind its arrival)."""
-    pinned = xs.is_pinned()
+    completions.  Outputs go to consecutive slices of `arena` (one is made when
+    none is given; it must hold every output of the trace).  Returns
+    (completions by ticket, outputs by ticket or None, wall seconds from the
+    first arrival to the last completion, the largest lag of a submission
+    behind its arrival)."""
+    if arena is None:
+        arena = output_arena(trace, pin=xs.is_pinned())
     tickets, outs, comps = {}, {}, {}
+    off = 0
     start = time.perf_counter()
     lag = 0.0
     for k, r in enumerate(trace):
@@ -205,7 +217,9 @@ def replay(server: Server, trace: list[TraceRequest], xs: torch.Tensor, qs: torc
         s = r.system
         x = xs[r.offset:r.offset + 3 * s.N]
         q = qs[r.offset:r.offset + s.N]
-        out = torch.empty(s.out_width * s.N, dtype=torch.float64, pin_memory=pinned)
+        w = s.out_width * s.N
+        out = arena[off:off + w]
+        off += w
         t = server.submit(s, x, q, out)
         tickets[t] = k
         if keep_outputs:
