@@ -108,6 +108,16 @@ const char* se_gpu_error_detail(void);
 int se_plan_set_timing(se_plan plan, int on);
 int se_plan_stage_ms(se_plan plan, float ms[4]);
 
+/* CUDA graphs for repeated solves (a time-stepping caller that solves the
+ * same buffers again and again).  With graphs on, the first solve runs
+ * directly, the second is captured into a graph and every later solve with
+ * the same buffers, stream and particle count replays it; other buffers, a
+ * new N or timing switched on or off capture a new graph.  System parameters
+ * (L, xi, m via se_solve_system) may change between replays.  Solves on the
+ * legacy default stream always run directly.  Results are identical either
+ * way. */
+int se_plan_set_graph(se_plan plan, int on);
+
 /* FP32 FMA throughput (TFLOP/s) of the current GPU from an FMA-chain kernel:
  * the compute roofline of the spread and interpolation kernels. */
 int se_probe_fma_tflops(double* tflops, void* stream);
@@ -162,6 +172,8 @@ int se_batch_solve(se_batch batch, const double* x, const double* q, double* out
 int se_batch_launch_count(se_batch batch);
 int se_batch_set_timing(se_batch batch, int on);
 int se_batch_stage_ms(se_batch batch, float ms[4]);
+/* The same CUDA-graph replay as se_plan_set_graph, for a batch. */
+int se_batch_set_graph(se_batch batch, int on);
 
 /* Solve one system on a plan made for the same M, P and mode, with the
  * system's own N (<= the plan's max_particles), L, xi and m.  The plan's

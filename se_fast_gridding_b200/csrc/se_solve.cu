@@ -311,6 +311,15 @@ struct se_batch_s {
     // per-stage CUDA events (prepare+sort, spread, k-space, interp)
     bool timing = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // CUDA graph of one solve (se_*_set_graph): captured on the second solve
+    // with the same buffers, stream and particle count, replayed after that
+    bool graph_on = false;
+    bool graph_warm = false;
+    cudaGraphExec_t gexec = nullptr;
+    const void* gkey[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t gstream = nullptr;
+    int gntot = -1, glaunches = 0;
+    bool gtiming = false;
 };
 
 namespace se {
@@ -431,9 +440,17 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     return b;
 }
 
+static void graph_drop(se_batch b)
+{
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+    b->graph_warm = false;
+}
+
 static int batch_free(se_batch b)
 {
     if (!b) return SE_OK;
+    graph_drop(b);
     for (auto& g : b->groups) {
         if (g.fwd) cufftDestroy(g.fwd);
         if (g.bwd) cufftDestroy(g.bwd);
@@ -889,8 +906,8 @@ static int run_interp(se_batch b, const double* grid, double* out, double* phi, 
     return SE_OK;
 }
 
-static int batch_solve(se_batch b, const double* x, const double* q, double* out, double* phi,
-                       cudaStream_t st)
+static int batch_solve_direct(se_batch b, const double* x, const double* q, double* out,
+                              double* phi, cudaStream_t st)
 {
     b->launches = b->pending_launches;
     b->pending_launches = 0;
@@ -908,6 +925,65 @@ static int batch_solve(se_batch b, const double* x, const double* q, double* out
     SE_TRY(mark(3));
     SE_TRY(run_interp(b, b->grid, out, phi, st));
     SE_TRY(mark(4));
+    return SE_OK;
+}
+
+// A solve through the batch's CUDA graph when graphs are on: the launch
+// sequence of a solve depends only on the buffers, the stream and the
+// particle count (the systems' parameters are read from the device table),
+// so a graph captured once replays every later solve with the same ones.
+// The legacy default streams cannot be captured: solves there run directly.
+static int batch_solve(se_batch b, const double* x, const double* q, double* out, double* phi,
+                       cudaStream_t st)
+{
+    const bool capturable = st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
+    if (!b->graph_on || !capturable) return batch_solve_direct(b, x, q, out, phi, st);
+    const bool same = b->gstream == st && b->gkey[0] == x && b->gkey[1] == q &&
+                      b->gkey[2] == out && b->gkey[3] == phi && b->gntot == b->ntot &&
+                      b->gtiming == b->timing;
+    if (!same) {
+        graph_drop(b);
+        b->gstream = st;
+        b->gkey[0] = x;
+        b->gkey[1] = q;
+        b->gkey[2] = out;
+        b->gkey[3] = phi;
+        b->gntot = b->ntot;
+        b->gtiming = b->timing;
+    }
+    if (!b->gexec && !b->graph_warm) {   // first solve: direct (sets up kernel attributes)
+        b->graph_warm = true;
+        return batch_solve_direct(b, x, q, out, phi, st);
+    }
+    const int pending = b->pending_launches;
+    b->pending_launches = 0;
+    if (!b->gexec) {
+        SE_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int r = batch_solve_direct(b, x, q, out, phi, st);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (r != SE_OK) {
+            if (g) cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+        const cudaError_t ei = cudaGraphInstantiate(&b->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            b->gexec = nullptr;
+            return cuda_fail(ei, "cudaGraphInstantiate", __FILE__, __LINE__);
+        }
+        b->glaunches = b->launches;
+    }
+    SE_CUDA(cudaGraphLaunch(b->gexec, st));
+    b->launches = pending + b->glaunches;
+    return SE_OK;
+}
+
+static int set_graph(se_batch b, int on)
+{
+    if (!on) graph_drop(b);
+    b->graph_on = on != 0;
     return SE_OK;
 }
 
@@ -1185,6 +1261,16 @@ extern "C" int se_batch_solve(se_batch b, const double* x, const double* q, doub
 }
 
 extern "C" int se_batch_launch_count(se_batch b) { return b ? b->launches : 0; }
+
+extern "C" int se_plan_set_graph(se_plan p, int on)
+{
+    return p ? set_graph(p->b, on) : SE_ERR_INVALID;
+}
+
+extern "C" int se_batch_set_graph(se_batch b, int on)
+{
+    return b ? set_graph(b, on) : SE_ERR_INVALID;
+}
 
 extern "C" int se_plan_set_timing(se_plan p, int on)
 {

@@ -18,8 +18,8 @@
 // 4 y planes, and each lane adds px[x] * (py[y] pz[z]) into 16 x 2 cells (all
 // 16 x of its (y, z) and (y, z + 1)).  Every cell is written once: no atomics
 // and a fixed order of summation.  FP32: fma.rn.f32x2 on the packed cells,
-// and after every 64 particles the FP32 sums are added into FP64 in shared
-// memory.
+// and after every 128 particles (two chunks) the FP32 sums are added into
+// FP64 in shared memory.
 
 constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
@@ -32,9 +32,6 @@ struct Spread2Smem {
     Acc px[S2_CHUNK][16];
     Acc py[S2_CHUNK][16];
     Acc pz[S2_CHUNK][16];
-    Acc cq[S2_CHUNK];
-    int cpart[S2_CHUNK];
-    int chalf[S2_CHUNK];
     unsigned ymask[S2_CHUNK];
     int list[S2_WARPS][S2_CHUNK];
     int ring[S2_RING];
@@ -187,7 +184,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
         for (int c = 0; c < 32; c++) sm.fold[c][t] = 0.0;
     const unsigned pmask = (P >= 32) ? 0xffffffffu : ((1u << P) - 1u);
 
-    int head = 0, tail = 0;
+    int head = 0, tail = 0, nfold = 0;
     for (int cb = 0; cb < total; cb += S2_THREADS) {
         __syncthreads();   // segment table ready; wsum free
         // ---- candidates: keep the particles whose stencil meets the tile
@@ -225,29 +222,18 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
         while (tail - head >= S2_CHUNK || (last && tail > head)) {
             const int n = min(S2_CHUNK, tail - head);
             __syncthreads();   // ring written; previous chunk's rows consumed
-            if (t < n) {
-                const int p = sm.ring[(head + t) & (S2_RING - 1)];
-                const int pk = sg[p];
-                const int gy = g_of(pk, 1);
-                const int hx = tile_half(g_of(pk, 0), tix, nt, P);
-                const int hy = tile_half(gy, tiy, nt, P);
-                const int hz = tile_half(g_of(pk, 2), tiz, nt, P);
-                sm.cpart[t] = p;
-                sm.chalf[t] = hx | (hy << 1) | (hz << 2);
-                sm.ymask[t] = ((pmask << (gy & 15)) >> (16 * hy)) & 0xFFFFu;
-                sm.cq[t] = (Acc)srec[p].w;
-            }
-            __syncthreads();
-            // tile rows: item (axis, particle), a 16-entry aligned copy each
             for (int it = t; it < 3 * n; it += S2_THREADS) {
                 const int a = it / n, p = it - a * n;
-                const int h = (sm.chalf[p] >> a) & 1;
-                const Acc* src = rows + ((long long)sm.cpart[p] * 3 + a) * 32 + 16 * h;
+                const int part = sm.ring[(head + p) & (S2_RING - 1)];
+                const int ga = g_of(sg[part], a);
+                const int h = tile_half(ga, a == 0 ? tix : (a == 1 ? tiy : tiz), nt, P);
+                if (a == 1) sm.ymask[p] = ((pmask << (ga & 15)) >> (16 * h)) & 0xFFFFu;
+                const Acc* src = rows + ((long long)part * 3 + a) * 32 + 16 * h;
                 Acc* dst = a == 0 ? sm.px[p] : (a == 1 ? sm.py[p] : sm.pz[p]);
                 if constexpr (sizeof(Acc) == 4) {
                     const float4* s4 = reinterpret_cast<const float4*>(src);
                     float4* d4 = reinterpret_cast<float4*>(dst);
-                    const float qw = a == 0 ? sm.cq[p] : 1.0f;
+                    const float qw = a == 0 ? (float)srec[part].w : 1.0f;
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
                         float4 v = __ldg(s4 + k);
@@ -257,7 +243,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
                 } else {
                     const double2* s2 = reinterpret_cast<const double2*>(src);
                     double2* d2 = reinterpret_cast<double2*>(dst);
-                    const double qw = a == 0 ? sm.cq[p] : 1.0;
+                    const double qw = a == 0 ? srec[part].w : 1.0;
 #pragma unroll
                     for (int k = 0; k < 8; k++) {
                         double2 v = __ldg(s2 + k);
@@ -266,6 +252,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
                     }
                 }
             }
+            __syncthreads();
             // this warp's particles: y rows meeting its 4 y planes
             int cnt = 0;
             for (int base = 0; base < n; base += 32) {
@@ -275,18 +262,19 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
                 if (act) sm.list[warp][cnt + __popc(bits & ((1u << lane) - 1u))] = q;
                 cnt += __popc(bits);
             }
-            __syncthreads();
+            __syncwarp();
             for (int i = 0; i < cnt; i++) {
                 const int p = sm.list[warp][i];
                 const Acc y = sm.py[p][ly];
                 const Acc c0 = y * sm.pz[p][lz], c1 = y * sm.pz[p][lz + 1];
                 acc.add(sm.px[p], c0, c1);
             }
-            if (FOLD) acc.fold(sm, t);
+            if (FOLD && (++nfold & 1) == 0) acc.fold(sm, t);
             head += n;
         }
     }
 
+    if (FOLD) acc.fold(sm, t);
     // ---- write the tile: 16 x of (y, z) and (y, z + 1) per lane
     double* gs = grid + S.grid_off;
     const long long row = ((long long)(y0 + ly)) * M + z0 + lz;

@@ -165,6 +165,11 @@ class SpectralEwald:
     def set_timing(self, on: bool = True) -> None:
         check(lib().se_plan_set_timing(self._plan, int(on)), "se_plan_set_timing")
 
+    def set_graph(self, on: bool = True) -> None:
+        """Replay repeated solves on the same buffers from a CUDA graph
+        (se_plan_set_graph)."""
+        check(lib().se_plan_set_graph(self._plan, int(on)), "se_plan_set_graph")
+
     def stage_ms(self) -> dict:
         """CUDA-event milliseconds of the last solve's stages (timing on)."""
         ms = (C.c_float * 4)()
@@ -246,6 +251,9 @@ class BatchSolver:
 
     def set_timing(self, on: bool = True) -> None:
         check(lib().se_batch_set_timing(self._b, int(on)), "se_batch_set_timing")
+
+    def set_graph(self, on: bool = True) -> None:
+        check(lib().se_batch_set_graph(self._b, int(on)), "se_batch_set_graph")
 
     def stage_ms(self) -> dict:
         ms = (C.c_float * 4)()
