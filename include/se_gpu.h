@@ -118,6 +118,26 @@ int se_plan_stage_ms(se_plan plan, float ms[4]);
  * way. */
 int se_plan_set_graph(se_plan plan, int on);
 
+/* ------------------------------------------------- real space and self -- */
+/* The other two parts of the Ewald sum, for a cubic box of edge L (device
+ * buffers, accumulated into):
+ *   phi[m] += sum_n sum_p q[n] erfc(xi r)/r over the images p in
+ *   [-layers, layers]^3 with r = |x_m - x_n + p L|, the self image (m = n,
+ *   p = 0) left out and, for rc > 0, the pairs with r > rc
+ *   (SE3P_direct_real_rc, SE_direct.c:464-506; rc <= 0: SE3P_direct_real,
+ *   :508-549);
+ *   force[m + a N] += q[m] sum q[n] (erfc(xi r)/r + 2 xi/sqrt(pi)
+ *   exp(-xi^2 r^2)) r_a / r^2 over the same pairs: the force of that
+ *   potential (the reference has no real-space force).
+ * phi or force may be NULL (not both).  Cutoffs 0 < rc <= L/2 with at least
+ * three cells of edge >= rc per axis use a cell list (positions anywhere
+ * within +-511 boxes; scratch from the stream-ordered pool); the others all
+ * pairs, in the reference's order of summation. */
+int se_real_space(const double* x, const double* q, int N, double L, double xi, int layers,
+                  double rc, double* phi, double* force, void* stream);
+/* phi[m] -= 2 xi / sqrt(pi) q[m]: SE3P_direct_self (SE_direct.c:551-562). */
+int se_self_term(const double* q, int N, double xi, double* phi, void* stream);
+
 /* FP32 FMA throughput (TFLOP/s) of the current GPU from an FMA-chain kernel:
  * the compute roofline of the spread and interpolation kernels. */
 int se_probe_fma_tflops(double* tflops, void* stream);

@@ -291,6 +291,37 @@ def direct_fd(x, q, L, xi, layers):
     return phi
 
 
+def direct_real(x, q, L, xi, layers, rc=0.0, phi=None):
+    """Real-space Ewald potential (SE_direct.c:464-549): rc <= 0 no cutoff."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    out = np.zeros(len(q)) if phi is None else np.array(phi, dtype=np.float64)
+    box = np.array([L, L, L], dtype=np.float64)
+    lib().orc_direct_real(dptr(out), dptr(x), dptr(q), len(q), dptr(box), C.c_double(xi),
+                          int(layers), C.c_double(rc))
+    return out
+
+
+def direct_self(q, xi, phi=None):
+    """Self term phi -= 2 xi / sqrt(pi) q (SE_direct.c:551-562)."""
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    out = np.zeros(len(q)) if phi is None else np.array(phi, dtype=np.float64)
+    lib().orc_direct_self(dptr(out), dptr(q), len(q), C.c_double(xi))
+    return out
+
+
+def direct_real_force(x, q, L, xi, layers, rc=0.0):
+    """Force of the real-space potential (its gradient times -q; no
+    counterpart in the reference)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    out = np.zeros(3 * len(q))
+    box = np.array([L, L, L], dtype=np.float64)
+    lib().orc_direct_real_force(dptr(out), dptr(x), dptr(q), len(q), dptr(box),
+                                C.c_double(xi), int(layers), C.c_double(rc))
+    return out
+
+
 def direct_force_fd(x, q, L, xi, layers):
     N = len(q)
     f = np.zeros(3 * N)

@@ -631,3 +631,64 @@ void orc_reorder(double* x, double* q, const int* idx, int N)
     }
     free(keys); free(perm); free(offs); free(xc); free(qc);
 }
+
+/* SE_direct.c:464-506 (rc > 0) and :508-549 (rc <= 0): for every target the
+ * sources in index order, the images in (p0, p1, p2) nested order. */
+void orc_direct_real(double* phi, const double* x, const double* q, int N,
+                     const double box[3], double xi, int layers, double rc)
+{
+#pragma omp parallel for schedule(dynamic)
+    for (int m = 0; m < N; m++) {
+        double acc = 0;
+        for (int n = 0; n < N; n++) {
+            const double r0 = x[m] - x[n], r1 = x[m + N] - x[n + N],
+                         r2 = x[m + 2 * N] - x[n + 2 * N];
+            for (int p0 = -layers; p0 <= layers; p0++)
+                for (int p1 = -layers; p1 <= layers; p1++)
+                    for (int p2 = -layers; p2 <= layers; p2++) {
+                        if (m == n && p0 == 0 && p1 == 0 && p2 == 0) continue;
+                        const double a = r0 + p0 * box[0], b = r1 + p1 * box[1],
+                                     c = r2 + p2 * box[2];
+                        const double r = sqrt(a * a + b * b + c * c);
+                        if (rc > 0 && r > rc) continue;
+                        acc += q[n] * erfc(xi * r) / r;
+                    }
+        }
+        phi[m] += acc;
+    }
+}
+
+/* SE_direct.c:551-562 */
+void orc_direct_self(double* phi, const double* q, int N, double xi)
+{
+    const double c = 2 * xi / sqrt(ORC_PI);
+    for (int m = 0; m < N; m++) phi[m] -= c * q[m];
+}
+
+/* the gradient of orc_direct_real times -q[m] (the force on m), same pairs */
+void orc_direct_real_force(double* force, const double* x, const double* q, int N,
+                           const double box[3], double xi, int layers, double rc)
+{
+    const double g = 2 * xi / sqrt(ORC_PI);
+#pragma omp parallel for schedule(dynamic)
+    for (int m = 0; m < N; m++) {
+        double f[3] = {0, 0, 0};
+        for (int n = 0; n < N; n++) {
+            const double r0 = x[m] - x[n], r1 = x[m + N] - x[n + N],
+                         r2 = x[m + 2 * N] - x[n + 2 * N];
+            for (int p0 = -layers; p0 <= layers; p0++)
+                for (int p1 = -layers; p1 <= layers; p1++)
+                    for (int p2 = -layers; p2 <= layers; p2++) {
+                        if (m == n && p0 == 0 && p1 == 0 && p2 == 0) continue;
+                        const double d[3] = {r0 + p0 * box[0], r1 + p1 * box[1],
+                                             r2 + p2 * box[2]};
+                        const double rr = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                        const double r = sqrt(rr);
+                        if (rc > 0 && r > rc) continue;
+                        const double s = q[n] * (erfc(xi * r) / r + g * exp(-xi * xi * rr)) / rr;
+                        for (int a = 0; a < 3; a++) f[a] += s * d[a];
+                    }
+        }
+        for (int a = 0; a < 3; a++) force[m + a * N] += q[m] * f[a];
+    }
+}

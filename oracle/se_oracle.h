@@ -73,6 +73,18 @@ void orc_direct_fd(double* phi, const double* x, const double* q, int N,
                    const double box[3], double xi, int layers);
 void orc_direct_force_fd(double* force, const double* x, const double* q, int N,
                          const double box[3], double xi, int layers);
+/* real-space Ewald sums over the periodic images p in [-layers, layers]^3:
+ * phi[m] += sum_n sum_p q[n] erfc(xi r) / r, r = |x_m - x_n + p box|, the
+ * self image (m = n, p = 0) left out, pairs with r > rc left out when rc > 0
+ * (SE3P_direct_real_rc / SE3P_direct_real); self term phi[m] -= 2 xi/sqrt(pi)
+ * q[m] (SE3P_direct_self); the real-space force, the gradient of the same
+ * sum (no counterpart in the reference): force[m + aN] += q[m] sum q[n]
+ * (erfc(xi r)/r + 2 xi/sqrt(pi) exp(-xi^2 r^2)) r_a / r^2 */
+void orc_direct_real(double* phi, const double* x, const double* q, int N,
+                     const double box[3], double xi, int layers, double rc);
+void orc_direct_self(double* phi, const double* q, int N, double xi);
+void orc_direct_real_force(double* force, const double* x, const double* q, int N,
+                           const double box[3], double xi, int layers, double rc);
 /* the same sums through structure factors, O(K N); jmax: cube half-width,
  * kcut2 > 0 restricts to |k|^2 <= kcut2 (a converged sphere) */
 void orc_sf_kspace(const double* x, const double* q, int N, const double box[3],

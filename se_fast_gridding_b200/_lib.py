@@ -143,6 +143,9 @@ def lib() -> C.CDLL:
         "se_batch_stage_ms": (C.c_int, [_vp, C.POINTER(C.c_float * 4)]),
         "se_probe_fma_tflops": (C.c_int, [_dp, _vp]),
         "se_plan_set_graph": (C.c_int, [_vp, C.c_int]),
+        "se_real_space": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.c_double, _vp, _vp, _vp]),
+        "se_self_term": (C.c_int, [_vp, C.c_int, C.c_double, _vp, _vp]),
         "se_batch_set_graph": (C.c_int, [_vp, C.c_int]),
         "se_solve_system": (C.c_int, [_vp, C.POINTER(se_system), _vp, _vp, _vp, _vp, _vp]),
         "se_server_request_bytes": (C.c_size_t, [C.POINTER(se_system), C.c_int]),

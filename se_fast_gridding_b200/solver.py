@@ -298,3 +298,29 @@ def counting_sort(keys: torch.Tensor, nkeys: int, stream=None):
     check(lib().se_counting_sort(_ptr(keys), N, nkeys, _ptr(perm), _ptr(offs), _ptr(scratch),
                                  nb, _stream(stream)), "se_counting_sort")
     return perm[:N], offs
+
+
+def real_space(x: torch.Tensor, q: torch.Tensor, L: float, xi: float, layers: int = 1,
+               rc: float = 0.0, phi: torch.Tensor | None = None, force: torch.Tensor | None = None,
+               want_force: bool = False, stream=None):
+    """Real-space Ewald potential (and force) of a cubic box, accumulated into
+    phi / force (se_real_space; SE3P_direct_real_rc, SE_direct.c:464-506).
+    Returns (phi, force)."""
+    N = q.numel()
+    if phi is None:
+        phi = torch.zeros(N, dtype=torch.float64, device=q.device)
+    if want_force and force is None:
+        force = torch.zeros(3 * N, dtype=torch.float64, device=q.device)
+    check(lib().se_real_space(_ptr(x), _ptr(q), N, float(L), float(xi), int(layers), float(rc),
+                              _ptr(phi), _ptr(force), _stream(stream)), "se_real_space")
+    return phi, force
+
+
+def self_term(q: torch.Tensor, xi: float, phi: torch.Tensor | None = None,
+              stream=None) -> torch.Tensor:
+    """phi -= 2 xi / sqrt(pi) q (se_self_term; SE3P_direct_self)."""
+    if phi is None:
+        phi = torch.zeros(q.numel(), dtype=torch.float64, device=q.device)
+    check(lib().se_self_term(_ptr(q), q.numel(), float(xi), _ptr(phi), _stream(stream)),
+          "se_self_term")
+    return phi

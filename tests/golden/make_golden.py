@@ -204,9 +204,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--skip-c2", action="store_true")
+    ap.add_argument("--realspace-only", action="store_true")
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}", "all", "ref"],
                    check=True)
+    if args.realspace_only:
+        return realspace(Ref("pot"), atoms(args.ref))
     ref = Ref("pot")
     reff = Ref("force")
     ref2p = Ref("2p")
@@ -292,6 +295,7 @@ def main():
     np.savez_compressed(os.path.join(OUT, "c1.npz"), **out)
     print("c1.npz: rel-RMS SE vs direct", O.rel_rms(out["phi_ref"], phi_d))
 
+    realspace(ref, A)
     if args.skip_c2:
         return
     # ---------------- 4. C2: FORCE N=1e5, M=128, P=16, xi=20 (1000-particle subset)
@@ -314,6 +318,39 @@ def main():
     np.savez_compressed(os.path.join(OUT, "c2.npz"), **out)
     print("c2.npz: rel-RMS SE force vs direct", O.rel_rms(out["force_ref"], f_d),
           "phi", O.rel_rms(out["phi_ref"], phi_d))
+
+
+def realspace(ref, A):
+    """5. The real-space and self terms: SE3P_direct_real_rc
+    (SE_direct.c:464-506), SE3P_direct_real (:508-549), SE3P_direct_self
+    (:551-562) on atoms.txt (N=100, L=3.1814) and a seeded N=400 unit-box
+    system."""
+    out = {}
+    Lb = 3.1814
+    xa = O.aligned_copy(A[:100, :3].T.reshape(-1))
+    qa = O.aligned_copy(A[:100, 3])
+    xs, qs = O.synthetic_system(400, 1.0, seed=21, charges="uniform")
+    xs, qs = O.aligned_copy(xs), O.aligned_copy(qs)
+    cases = [("atoms_l1_rc1.5", xa, qa, Lb, 2.0, 1, 1.5), ("atoms_l0_rc1.2", xa, qa, Lb, 2.0, 0, 1.2),
+             ("atoms_l1_nocut", xa, qa, Lb, 3.0, 1, 0.0), ("atoms_l2_rc2", xa, qa, Lb, 1.5, 2, 2.0),
+             ("syn_l1_rc0.35", xs, qs, 1.0, 9.0, 1, 0.35), ("syn_l1_rc0.5", xs, qs, 1.0, 7.0, 1, 0.5)]
+    out["atoms/x"], out["atoms/q"], out["syn/x"], out["syn/q"] = xa, qa, xs, qs
+    for tag, x, q, L, xi, layers, rc in cases:
+        N = len(q)
+        e = _ewald_opts(L, xi, layers)
+        e.rc = rc
+        phi = O.aligned_zeros(N)
+        if rc > 0:
+            ref.lib.SE3P_direct_real_rc(O.dptr(phi), O.dptr(x), O.dptr(q), N, e)
+        else:
+            ref.lib.SE3P_direct_real(O.dptr(phi), O.dptr(x), O.dptr(q), N, e)
+        out[f"{tag}/params"] = np.array([L, xi, layers, rc])
+        out[f"{tag}/phi"] = np.array(phi)
+        self_ = O.aligned_zeros(N)
+        ref.lib.SE3P_direct_self(O.dptr(self_), O.dptr(q), N, e)
+        out[f"{tag}/self"] = np.array(self_)
+    np.savez_compressed(os.path.join(OUT, "realspace.npz"), **out)
+    print("realspace.npz", len(out), "arrays")
 
 
 class _EwaldOpts(C.Structure):

@@ -167,3 +167,41 @@ def test_reorder_matches_reference(oracle_mod):
     # the oracle keeps ties in input order (stable)
     order = np.argsort(idx, kind="stable")
     np.testing.assert_array_equal(q, g["reorder/q_in"][order])
+
+
+REAL_CASES = ["atoms_l1_rc1.5", "atoms_l0_rc1.2", "atoms_l1_nocut", "atoms_l2_rc2",
+              "syn_l1_rc0.35", "syn_l1_rc0.5"]
+
+
+@pytest.mark.parametrize("tag", REAL_CASES)
+def test_oracle_real_space_and_self_match_reference(oracle_mod, tag):
+    """SE3P_direct_real_rc / SE3P_direct_real / SE3P_direct_self
+    (SE_direct.c:464-562) against the reference's own outputs."""
+    O = oracle_mod
+    g = load_golden("realspace.npz")
+    src = "atoms" if tag.startswith("atoms") else "syn"
+    x, q = g[f"{src}/x"], g[f"{src}/q"]
+    L, xi, layers, rc = g[f"{tag}/params"]
+    phi = O.direct_real(x, q, L, xi, int(layers), rc)
+    assert O.rel_rms(phi, g[f"{tag}/phi"]) < EXACT
+    np.testing.assert_allclose(O.direct_self(q, xi), g[f"{tag}/self"], rtol=1e-15, atol=0)
+
+
+def test_oracle_real_space_force_is_the_gradient(oracle_mod):
+    """The real-space force (no reference counterpart) is -q_m times the
+    gradient of the real-space potential at x_m: central differences."""
+    O = oracle_mod
+    x, q = O.synthetic_system(40, 1.0, seed=4, charges="uniform")
+    L, xi, layers, rc = 1.0, 6.0, 1, 0.0
+    f = O.direct_real_force(x, q, L, xi, layers, rc)
+    N, h = len(q), 1e-6
+    for m in (0, 7, 31):
+        for a in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[m + a * N] += h
+            xm[m + a * N] -= h
+            # energy of particle m only: phi_m(x) q_m (the pair terms' other
+            # half acts on the partner)
+            dphi = (O.direct_real(xp, q, L, xi, layers, rc)[m] -
+                    O.direct_real(xm, q, L, xi, layers, rc)[m]) / (2 * h)
+            assert abs(f[m + a * N] - (-q[m] * dphi)) < 1e-6 * max(1.0, abs(f[m + a * N]))
