@@ -69,11 +69,47 @@ typedef struct se_plan_s* se_plan;
 int se_config_derive(const se_config* cfg, double* h, double* w, double* eta,
                      double* c, double* d);
 
+/* Parameters for an accuracy target (no GPU needed).  The reference's
+ * SE_init_params (SE_general.c:517-572) takes P as given and prints the
+ * Lindbo-Tornberg estimate of the absolute RMS error; this picks the
+ * smallest P (<= 32) whose estimate is <= eps for the charges' sum of
+ * squares Q in the given mode, m = 0.95 sqrt(pi P), and the reference's
+ * Kolafa-Perram grid M = ceil(4 xi L + 1) + 2 (at least P), rounded up to a
+ * multiple of 16 from 32 on (the tile-aligned kernels) and to even below.
+ * SE_ERR_UNSUPPORTED when no P <= 32 or M <= 1024 reaches eps. */
+int se_choose_params(double eps, double L, double xi, double Q, int mode, int* M, int* P,
+                     double* m);
+/* The estimate itself for a given P (SE_init_params' "bound for potential"
+ * or "bound for force"). */
+double se_error_estimate(int P, double L, double xi, double Q, int mode);
+
 /* Device bytes a plan of this configuration holds (admission control). */
 size_t se_plan_device_bytes(const se_config* cfg);
 
 int se_plan_create(se_plan* plan, const se_config* cfg);
 int se_plan_destroy(se_plan plan);
+
+/* Kernel paths (se_plan_create_ex): which spread and interpolation kernels a
+ * plan runs.  SE_PATH_TILE_SPREAD and SE_PATH_PAIR_INTERP need M a multiple
+ * of 16, M >= 32 and P <= 16; SE_PATH_RUNTIME_P turns off the interpolation
+ * kernels specialised for P = 8, 12, 16 (21).  SE_PATH_DEFAULT is what
+ * se_plan_create does (both tile kernels where they apply); SE_PATH_TUNE times
+ * every valid path on the plan's configuration (synthetic uniform particles,
+ * N = max_particles, at most 2^20) and keeps the fastest, remembered per
+ * (M, P, mode, precision, power-of-two class of N) for the process and, with
+ * the environment variable SE_GPU_TUNE_FILE set, in that file.  Every path
+ * meets the same accuracy; different paths sum in different orders, so their
+ * results differ in the last bits.  se_plan_device_bytes reports the default
+ * path; a path mixing tile and general kernels holds 3P more factors per
+ * particle. */
+#define SE_PATH_DEFAULT (-1)
+#define SE_PATH_TUNE (-2)
+#define SE_PATH_TILE_SPREAD 1
+#define SE_PATH_PAIR_INTERP 2
+#define SE_PATH_RUNTIME_P 4
+int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path);
+/* The path a plan runs (SE_PATH_* bits). */
+int se_plan_path(se_plan plan);
 
 /* Full k-space solve on device buffers.  out: N (POTENTIAL) or 3N (FORCE).
  * phi_out (may be NULL) additionally receives the potential in FORCE mode. */

@@ -87,6 +87,8 @@ class se_server_stats(C.Structure):
 SE_OK, SE_ERR_CUDA, SE_ERR_INVALID, SE_ERR_UNSUPPORTED, SE_ERR_NOMEM, SE_ERR_CUFFT, \
     SE_ERR_INPUT, SE_ERR_BUSY, SE_ERR_TIMEOUT = range(9)
 SE_WHERE_HOST, SE_WHERE_DEVICE = 0, 1
+SE_PATH_DEFAULT, SE_PATH_TUNE = -1, -2
+SE_PATH_TILE_SPREAD, SE_PATH_PAIR_INTERP, SE_PATH_RUNTIME_P = 1, 2, 4
 SE_POTENTIAL, SE_FORCE = 0, 1
 SE_FP64, SE_FP32 = 0, 1
 
@@ -143,6 +145,12 @@ def lib() -> C.CDLL:
         "se_batch_stage_ms": (C.c_int, [_vp, C.POINTER(C.c_float * 4)]),
         "se_probe_fma_tflops": (C.c_int, [_dp, _vp]),
         "se_plan_set_graph": (C.c_int, [_vp, C.c_int]),
+        "se_plan_create_ex": (C.c_int, [C.POINTER(_vp), C.POINTER(se_config), C.c_int]),
+        "se_plan_path": (C.c_int, [_vp]),
+        "se_choose_params": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       _ip, _ip, _dp]),
+        "se_error_estimate": (C.c_double, [C.c_int, C.c_double, C.c_double, C.c_double,
+                                           C.c_int]),
         "se_real_space": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, C.c_int,
                                     C.c_double, _vp, _vp, _vp]),
         "se_self_term": (C.c_int, [_vp, C.c_int, C.c_double, _vp, _vp]),

@@ -33,11 +33,23 @@ __device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsign
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
     return d;
 }
-// A system's spread runs in k_spread2 (tile-aligned factor rows) when its
-// grid is cut into whole 16^3 tiles and its stencil fits two tiles.
+// The tile-aligned kernels (k_spread2, k_interp2 on tile-aligned factor rows)
+// apply when a system's grid is cut into whole 16^3 tiles and its stencil
+// fits two tiles.
 __host__ __device__ inline bool spread2_eligible(int M, int P)
 {
     return M % 16 == 0 && M >= 32 && P <= 16;
+}
+
+// A system's kernel path (SysDev::path): which spread and interpolation run.
+constexpr int PATH_TILE_SPREAD = 1;    // k_spread2 (else k_spread)
+constexpr int PATH_PAIR_INTERP = 2;    // k_interp2 (else k_interp / k_interp_global)
+constexpr int PATH_RUNTIME_P = 4;      // interpolation without the P-unrolled variants
+
+// The default path: the tile-aligned kernels wherever they apply.
+__host__ __device__ inline int default_path(int M, int P)
+{
+    return spread2_eligible(M, P) ? PATH_TILE_SPREAD | PATH_PAIR_INTERP : 0;
 }
 
 constexpr int MAX_SEG = 96;               // bin segments reaching one tile
@@ -48,6 +60,7 @@ constexpr double PI_D = 3.14159265358979323846;
 // Per-system parameters and offsets of a batch (one entry per system).
 struct SysDev {
     int N, M, P, lo, mode;
+    int path;         // PATH_* bits
     int part_off, out_off;
     long long grid_off, spec_off;
     int nf[3];        // fine bins per axis

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp(
     const int beg = boff[bin], end = boff[bin + 1];
     if (beg == end) return;
     const SysDev& S = sys[find_sys(bin_prefix, nsys, bin)];
-    if (rows && spread2_eligible(S.M, S.P)) return;   // k_interp2 covers this system
+    if (S.path & PATH_PAIR_INTERP) return;   // k_interp2 covers this system
     const int P = PT ? PT : S.P;
     const int M = S.M;
     const int lb = bin - S.bin_base;
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(INTERP_WARPS * 32) k_interp_global(
     if (p >= ntot) return;
     const int orig = sperm[p];
     const SysDev& S = sys[find_sys(part_prefix, nsys, orig)];
-    if (rows && spread2_eligible(S.M, S.P)) return;   // k_interp2 covers this system
+    if (S.path & PATH_PAIR_INTERP) return;   // k_interp2 covers this system
     const int P = S.P, M = S.M;
     InterpWarpSmem<T>& W = wsm[warp];
     const double4 rc = srec[p];

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(I2_WARPS * 32) k_interp2(
     const int beg = boff[bin], end = boff[bin + 1];
     if (beg == end) return;
     const SysDev& S = sys[find_sys(bin_prefix, nsys, bin)];
-    if (!spread2_eligible(S.M, S.P)) return;   // k_interp covers this system
+    if (!(S.path & PATH_PAIR_INTERP)) return;   // k_interp covers this system
     const int P = PT ? PT : S.P;
     const int M = S.M;
     const int lb = bin - S.bin_base;

@@ -21,9 +21,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "se_internal.h"
@@ -112,7 +114,7 @@ __global__ void k_gather(int ntot, const int* __restrict__ perm, const double4* 
 // full Gaussian): v_0 = exp(-c u_0^2), r_0 = exp(2 c h u_0 - c h^2),
 // v_{i+1} = v_i r_i, r_{i+1} = r_i exp(-2 c h^2), u_0 = t0 - lo h, stored in
 // the working precision T.  Thread u = 3 s + a writes particle s, axis a:
-//  - systems k_spread2 serves (spread2_eligible): the tile-aligned 32-entry
+//  - systems on a tile-aligned kernel (PATH_TILE_SPREAD / PATH_PAIR_INTERP): the tile-aligned 32-entry
 //    row rows[u*32 + j] = f[j - (g_a mod 16)], zero outside the stencil; the
 //    rows of a warp are contiguous, so they are staged in shared memory and
 //    stored as one coalesced block;
@@ -140,8 +142,12 @@ __global__ void __launch_bounds__(factors_threads<T>()) k_factors(
         const double u0 = t0 - S.lo * S.h;
         double v = exp(-S.c * u0 * u0);
         double r = exp(2.0 * S.c * S.h * u0 - S.c * S.h * S.h);
-        if (rows && spread2_eligible(S.M, S.P)) {
+        const int tiled = S.path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP);
+        if (tiled) {
             staged = true;
+            // a path that mixes tile-aligned and general kernels needs both rows
+            T* f = tiled != (PATH_TILE_SPREAD | PATH_PAIR_INTERP) ? fac + (long long)u * PS
+                                                                  : nullptr;
             T* st = stage[threadIdx.x];
 #pragma unroll
             for (int j = 0; j < 32; j += V)
@@ -149,6 +155,7 @@ __global__ void __launch_bounds__(factors_threads<T>()) k_factors(
             st += ((unsigned)sg[s] >> (10 * a)) & 15u;
             for (int i = 0; i < S.P; i++) {
                 st[i] = (T)v;
+                if (f) f[i] = (T)v;
                 v *= r;
                 r *= S.rho;
             }
@@ -290,7 +297,9 @@ struct se_batch_s {
     void* fac = nullptr;      // per-particle factors [ntot][3][PS], working precision
     int PS = 0;
     void* rows = nullptr;     // tile-aligned rows [ntot][3][32] (k_spread2 systems)
-    bool any_spread1 = false, any_spread2 = false;
+    bool any_spread1 = false, any_spread2 = false;   // some system on k_spread / k_spread2
+    bool any_interp1 = false, any_interp2 = false;   // on k_interp(_global) / k_interp2
+    bool runtime_p = false;                          // some system asks for runtime P
     float* grid32 = nullptr;  // FP32 copy of the grids, staged by k_interp2<float>
     int i2_P = 0;             // largest P of the k_interp2 systems (0: none)
     bool i2_uniform = false;  // all k_interp2 systems have P == i2_P
@@ -359,6 +368,7 @@ static void fill_sysdev(const se_system& s, SysDev& S)
     S.P = s.P;
     S.lo = (s.P & 1) ? -ph : -ph + 1;
     S.mode = s.mode;
+    S.path = default_path(s.M, s.P);
     const int nf = (s.M + FB - 1) / FB;
     S.nf[0] = S.nf[1] = S.nf[2] = nf;
     S.nt[0] = (s.M + TX - 1) / TX;
@@ -404,8 +414,13 @@ static size_t interp_smem_bytes(int P, int precision)
     return (size_t)E * interp_plane(P) * (precision == SE_FP32 ? 4 : 8);
 }
 
+static int path_of(const se_system* sys, const int* paths, int i)
+{
+    return paths ? paths[i] : default_path(sys[i].M, sys[i].P);
+}
+
 static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nbins_out,
-                          int* ntiles_out)
+                          int* ntiles_out, const int* paths = nullptr)
 {
     long long ntot = 0, nbins = 0, ntiles = 0, grid = 0, spec = 0;
     for (int i = 0; i < nsys; i++) {
@@ -423,14 +438,16 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     b += (size_t)ntot * (4 + 32 + 4 + 4 + 32 + 4);
     int maxP = 1;
     for (int i = 0; i < nsys; i++) maxP = std::max(maxP, sys[i].P);
-    bool rows = false, plain = false;
+    bool rows = false, plain = false, pair = false;
     for (int i = 0; i < nsys; i++) {
-        if (spread2_eligible(sys[i].M, sys[i].P)) rows = true;
-        else plain = true;
+        const int t = path_of(sys, paths, i) & (PATH_TILE_SPREAD | PATH_PAIR_INTERP);
+        if (t) rows = true;
+        if (t != (PATH_TILE_SPREAD | PATH_PAIR_INTERP)) plain = true;
+        if (t & PATH_PAIR_INTERP) pair = true;
     }
     if (plain) b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
     if (rows) b += (size_t)ntot * 3 * 32 * (precision == SE_FP32 ? 4 : 8);
-    if (rows && precision == SE_FP32) b += (size_t)grid * 4;   // FP32 copy of the grids
+    if (pair && precision == SE_FP32) b += (size_t)grid * 4;   // FP32 copy of the grids
     b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
     b += (size_t)(nbins + 1) * 4;
     b += (size_t)grid * 8 + (size_t)spec * 16;
@@ -481,6 +498,7 @@ static const void* staged_interp_variant(int P, bool uniform)
 
 static bool uniform_P(const se_batch_s* b)
 {
+    if (b->runtime_p) return false;   // the runtime-P variants were asked for
     for (auto& s : b->host_sys)
         if (s.P != b->max_P) return false;
     return true;
@@ -559,12 +577,19 @@ static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
     *PL_out = best_PL;
 }
 
-static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision)
+static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision,
+                        const int* paths = nullptr)
 {
     if (!out || !systems || nsys < 1 || (precision != SE_FP64 && precision != SE_FP32))
         return SE_ERR_INVALID;
-    for (int i = 0; i < nsys; i++)
+    for (int i = 0; i < nsys; i++) {
         if (!valid_system(systems[i])) return SE_ERR_INVALID;
+        const int path = path_of(systems, paths, i);
+        if (path < 0 || path > 7 ||
+            ((path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP)) &&
+             !spread2_eligible(systems[i].M, systems[i].P)))
+            return SE_ERR_INVALID;
+    }
     se_batch b = new se_batch_s();
     b->nsys = nsys;
     b->precision = precision;
@@ -605,6 +630,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         SysDev& S = b->host_sys[i];
         memset(&S, 0, sizeof(S));
         fill_sysdev(s, S);
+        S.path = path_of(systems, paths, i);
         const int nf = S.nf[0];
         S.part_off = pcur;
         S.out_off = ocur;
@@ -653,18 +679,24 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     SE_ALLOC(b->sg, sizeof(int) * nt);
     SE_ALLOC(b->boff, sizeof(int) * (b->nbins + 1));
     b->PS = b->max_P;
+    bool need_fac = false, need_rows = false;
     for (int i = 0; i < nsys; i++) {
-        if (spread2_eligible(systems[i].M, systems[i].P)) b->any_spread2 = true;
-        else b->any_spread1 = true;
+        const int path = b->host_sys[i].path;
+        (path & PATH_TILE_SPREAD ? b->any_spread2 : b->any_spread1) = true;
+        (path & PATH_PAIR_INTERP ? b->any_interp2 : b->any_interp1) = true;
+        if (path & PATH_RUNTIME_P) b->runtime_p = true;
+        const int t = path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP);
+        if (t) need_rows = true;
+        if (t != (PATH_TILE_SPREAD | PATH_PAIR_INTERP)) need_fac = true;
     }
-    if (b->any_spread1) SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
-    if (b->any_spread2) SE_ALLOC(b->rows, nt * 3 * 32 * (precision == SE_FP32 ? 4 : 8));
-    if (b->any_spread2 && precision == SE_FP32)
+    if (need_fac) SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
+    if (need_rows) SE_ALLOC(b->rows, nt * 3 * 32 * (precision == SE_FP32 ? 4 : 8));
+    if (b->any_interp2 && precision == SE_FP32)
         SE_ALLOC(b->grid32, sizeof(float) * b->grid_elems);
-    if (b->any_spread2) {
+    if (b->any_interp2) {
         b->i2_uniform = true;
         for (int i = 0; i < nsys; i++) {
-            if (!spread2_eligible(systems[i].M, systems[i].P)) continue;
+            if (!(b->host_sys[i].path & PATH_PAIR_INTERP)) continue;
             if (b->i2_P && systems[i].P != b->i2_P) b->i2_uniform = false;
             b->i2_P = std::max(b->i2_P, systems[i].P);
         }
@@ -847,7 +879,7 @@ template <typename T>
 static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, cudaStream_t st)
 {
     const int P = b->i2_P;
-    const bool u = b->i2_uniform;
+    const bool u = b->i2_uniform && !b->runtime_p;
     const void* fn = (u && P == 8)    ? (const void*)k_interp2<T, 8>
                      : (u && P == 12) ? (const void*)k_interp2<T, 12>
                      : (u && P == 16) ? (const void*)k_interp2<T, 16>
@@ -872,7 +904,7 @@ static int run_interp(se_batch b, const double* grid, double* out, double* phi, 
     if (b->ntot == 0) return SE_OK;
     // systems of whole 16^3 tiles with P <= 16: k_interp2 (FP32 path from an
     // FP32 copy of the grids); the others: k_interp / k_interp_global
-    if (b->any_spread2) {
+    if (b->any_interp2) {
         if (b->precision == SE_FP32) {
             const long long n = b->grid_elems;
             k_grid_to_f32<<<std::min<long long>(4096, ceil_div(n / 2 + 1, 256)), 256, 0, st>>>(
@@ -885,7 +917,7 @@ static int run_interp(se_batch b, const double* grid, double* out, double* phi, 
             SE_TRY(launch_interp2<double>(b, grid, out, phi, st));
         }
     }
-    if (!b->any_spread1) return SE_OK;
+    if (!b->any_interp1) return SE_OK;
     if (b->staged_interp) {
         if (b->precision == SE_FP32) return launch_interp_staged<float>(b, grid, out, phi, st);
         return launch_interp_staged<double>(b, grid, out, phi, st);
@@ -1038,6 +1070,41 @@ struct se_plan_s {
 
 using namespace se;
 
+// The error estimate SE_init_params prints (SE_general.c:517-572), Lindbo &
+// Tornberg, for P points and c = m / sqrt(pi P) = 0.95.
+static double se_error_bound(int P, double L, double xi, double Q, int mode)
+{
+    const double c = 0.95;
+    const double g = exp(-PI_D * P * c * c / 2.);
+    if (mode == SE_FORCE) return Q * sqrt(xi * L) / (L * L) * g * 2. * PI_D * c * c * P;
+    return sqrt(Q * xi * L) / L * g;
+}
+
+extern "C" int se_choose_params(double eps, double L, double xi, double Q, int mode, int* M,
+                                int* P, double* m)
+{
+    if (!(eps > 0) || !(L > 0) || !(xi > 0) || !(Q >= 0) || !M || !P || !m ||
+        (mode != SE_POTENTIAL && mode != SE_FORCE))
+        return SE_ERR_INVALID;
+    int p = 2;
+    while (p < MAX_P && se_error_bound(p, L, xi, Q, mode) > eps) p++;
+    if (se_error_bound(p, L, xi, Q, mode) > eps) return SE_ERR_UNSUPPORTED;
+    // Kolafa & Perram: the grid resolves the k-space sum to k_inf = 2 xi L
+    int mm = (int)ceil(2. * (2. * xi * L) + 1.) + 2;
+    mm = std::max(mm, p);
+    mm = mm >= 32 ? (mm + 15) / 16 * 16 : (mm + 1) / 2 * 2;
+    if (mm > 1024) return SE_ERR_UNSUPPORTED;
+    *P = p;
+    *M = mm;
+    *m = 0.95 * sqrt(PI_D * p);
+    return SE_OK;
+}
+
+extern "C" double se_error_estimate(int P, double L, double xi, double Q, int mode)
+{
+    return se_error_bound(P, L, xi, Q, mode);
+}
+
 extern "C" int se_config_derive(const se_config* cfg, double* h, double* w, double* eta,
                                 double* c, double* d)
 {
@@ -1083,6 +1150,181 @@ extern "C" int se_plan_create(se_plan* plan, const se_config* cfg)
     return SE_OK;
 }
 
+// ---------------------------------------------------------------- tuning --
+// The kernel path of a plan chosen by timing: every valid path runs on the
+// plan's configuration with synthetic uniform particles (N = its capacity, at
+// most 2^20), and the fastest is kept in a process-wide table keyed by
+// (M, P, mode, precision, ceil(log2 N)); with SE_GPU_TUNE_FILE set, the table
+// is read from and appended to that file.
+
+__global__ void k_tune_fill(double* __restrict__ x, double* __restrict__ q, int N, double L)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    for (int a = 0; a < 3; a++) {
+        unsigned long long z = 0x9E3779B97F4A7C15ull * (3ull * n + a + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        x[n + (long long)a * N] = L * (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    }
+    q[n] = (n & 1) ? -1.0 : 1.0;
+}
+
+namespace {
+
+struct TuneKey {
+    int M, P, mode, precision, nclass;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(M, P, mode, precision, nclass) <
+               std::tie(o.M, o.P, o.mode, o.precision, o.nclass);
+    }
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+bool g_tune_loaded = false;
+
+const char* tune_file() { return getenv("SE_GPU_TUNE_FILE"); }
+
+void tune_load()
+{
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* f = tune_file();
+    if (!f) return;
+    FILE* fp = fopen(f, "r");
+    if (!fp) return;
+    TuneKey k;
+    int path;
+    while (fscanf(fp, "%d %d %d %d %d %d", &k.M, &k.P, &k.mode, &k.precision, &k.nclass,
+                  &path) == 6)
+        if (path >= 0 && path <= 7) g_tune[k] = path;
+    fclose(fp);
+}
+
+void tune_store(const TuneKey& k, int path)
+{
+    const char* f = tune_file();
+    if (!f) return;
+    FILE* fp = fopen(f, "a");
+    if (!fp) return;
+    fprintf(fp, "%d %d %d %d %d %d\n", k.M, k.P, k.mode, k.precision, k.nclass, path);
+    fclose(fp);
+}
+
+int tune_candidates(int M, int P, int* c)
+{
+    if (!spread2_eligible(M, P)) {
+        c[0] = 0;
+        c[1] = PATH_RUNTIME_P;
+        return 2;
+    }
+    const int all[6] = {PATH_TILE_SPREAD | PATH_PAIR_INTERP,
+                        PATH_TILE_SPREAD | PATH_PAIR_INTERP | PATH_RUNTIME_P,
+                        PATH_TILE_SPREAD, PATH_PAIR_INTERP, 0, PATH_RUNTIME_P};
+    for (int i = 0; i < 6; i++) c[i] = all[i];
+    return 6;
+}
+
+// Milliseconds of the fastest of 5 solves (after 2 untimed) on path `path`.
+int time_path(const se_system& s, int precision, int path, const double* x, const double* q,
+              double* out, cudaEvent_t e0, cudaEvent_t e1, float* best)
+{
+    se_batch b = nullptr;
+    SE_TRY(batch_create(&b, &s, 1, precision, &path));
+    int r = SE_OK;
+    *best = 1e30f;
+    for (int k = 0; k < 7 && r == SE_OK; k++) {
+        cudaEventRecord(e0, nullptr);
+        r = batch_solve_direct(b, x, q, out, nullptr, nullptr);
+        cudaEventRecord(e1, nullptr);
+        const cudaError_t e = cudaEventSynchronize(e1);
+        if (r == SE_OK && e != cudaSuccess) r = cuda_fail(e, "tuning solve", __FILE__, __LINE__);
+        float ms = 0;
+        if (r == SE_OK && k >= 2 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+            *best = std::min(*best, ms);
+    }
+    batch_free(b);
+    return r;
+}
+
+int tune_path(const se_config* cfg, int* path_out)
+{
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_load();
+    const int N = std::max(1, std::min(cfg->max_particles, 1 << 20));
+    int nclass = 0;
+    while ((1 << nclass) < std::max(cfg->max_particles, 1)) nclass++;
+    const TuneKey key{cfg->M, cfg->P, cfg->mode, cfg->precision, nclass};
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+        *path_out = it->second;
+        return SE_OK;
+    }
+    int cand[6];
+    const int nc = tune_candidates(cfg->M, cfg->P, cand);
+    se_system s = sys_of(cfg, N);
+    double *x = nullptr, *q = nullptr, *out = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&x, sizeof(double) * 3 * N);
+    if (e == cudaSuccess) e = cudaMalloc(&q, sizeof(double) * N);
+    if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(double) * 3 * N);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    int r = e == cudaSuccess ? SE_OK : cuda_fail(e, "tuning buffers", __FILE__, __LINE__);
+    if (r == SE_OK) {
+        k_tune_fill<<<ceil_div(N, 256), 256>>>(x, q, N, cfg->L);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) r = cuda_fail(e, "k_tune_fill", __FILE__, __LINE__);
+    }
+    int best_path = cand[0];
+    float best_ms = 1e30f;
+    for (int i = 0; i < nc && r == SE_OK; i++) {
+        float ms = 0;
+        r = time_path(s, cfg->precision, cand[i], x, q, out, e0, e1, &ms);
+        if (r == SE_OK && ms < best_ms) {
+            best_ms = ms;
+            best_path = cand[i];
+        }
+    }
+    if (x) cudaFree(x);
+    if (q) cudaFree(q);
+    if (out) cudaFree(out);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (r != SE_OK) return r;
+    g_tune[key] = best_path;
+    tune_store(key, best_path);
+    *path_out = best_path;
+    return SE_OK;
+}
+
+}  // namespace
+
+extern "C" int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path)
+{
+    if (!plan || !cfg || cfg->max_particles < 0) return SE_ERR_INVALID;
+    if (path == SE_PATH_DEFAULT) return se_plan_create(plan, cfg);
+    se_system s = sys_of(cfg, cfg->max_particles);
+    if (!valid_system(s) || (cfg->precision != SE_FP32 && cfg->precision != SE_FP64))
+        return SE_ERR_INVALID;
+    if (path == SE_PATH_TUNE) SE_TRY(tune_path(cfg, &path));
+    if (path < 0 || path > 7) return SE_ERR_INVALID;
+    se_plan p = new se_plan_s();
+    p->cfg = *cfg;
+    const int r = batch_create(&p->b, &s, 1, cfg->precision, &path);
+    if (r != SE_OK) {
+        delete p;
+        return r;
+    }
+    *plan = p;
+    return SE_OK;
+}
+
+extern "C" int se_plan_path(se_plan p) { return p ? p->b->host_sys[0].path : -1; }
+
 extern "C" int se_plan_destroy(se_plan p)
 {
     if (!p) return SE_OK;
@@ -1118,6 +1360,7 @@ static int plan_rebind(se_plan p, const se_system& s, cudaStream_t st)
     se_batch b = p->b;
     SysDev S = b->host_sys[0];
     fill_sysdev(s, S);
+    S.path = b->host_sys[0].path;   // the plan's kernel path stays
     if (memcmp(&S, &b->host_sys[0], sizeof(S)) == 0) return SE_OK;
     k_rebind<<<1, 32, 0, st>>>(b->sys, b->d_part_prefix, S);
     SE_CUDA(cudaGetLastError());

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, sizeof(Acc) == 4 ? 4 : 2) k_sp
 
     const int tile = blockIdx.x;
     const SysDev& S = sys[find_sys(tile_prefix, nsys, tile)];
-    if (spread2_eligible(S.M, S.P)) return;   // k_spread2 covers this system
+    if (S.path & PATH_TILE_SPREAD) return;   // k_spread2 covers this system
     const int lt = tile - S.tile_base;
     const int x0 = (lt / (S.nt[1] * S.nt[2])) * TX;
     const int y0 = ((lt / S.nt[2]) % S.nt[1]) * TY;

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
 
     const int tile = blockIdx.x;
     const SysDev& S = sys[find_sys(tile_prefix, nsys, tile)];
-    if (!spread2_eligible(S.M, S.P)) return;   // k_spread covers this system
+    if (!(S.path & PATH_TILE_SPREAD)) return;   // k_spread covers this system
     const int nt = S.nt[0], P = S.P, M = S.M;
     const int lt = tile - S.tile_base;
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;

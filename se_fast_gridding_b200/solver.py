@@ -64,6 +64,24 @@ class Params:
     d: float
 
 
+def choose_params(eps: float, L: float, xi: float, q, mode="potential") -> tuple[int, int, float]:
+    """(M, P, m) for an absolute RMS error target eps (se_choose_params): the
+    smallest P whose Lindbo-Tornberg estimate (SE_init_params,
+    SE_general.c:517-572) is <= eps, the Kolafa-Perram grid rounded for the
+    tile-aligned kernels.  q: the charges (or their sum of squares)."""
+    Q = float(q) if np.isscalar(q) else float(np.sum(np.asarray(q, dtype=np.float64) ** 2))
+    M, P, m = C.c_int(), C.c_int(), C.c_double()
+    check(lib().se_choose_params(float(eps), float(L), float(xi), Q, _mode(mode), C.byref(M),
+                                 C.byref(P), C.byref(m)), "se_choose_params")
+    return M.value, P.value, m.value
+
+
+def error_estimate(P: int, L: float, xi: float, q, mode="potential") -> float:
+    """The Lindbo-Tornberg error estimate SE_init_params prints."""
+    Q = float(q) if np.isscalar(q) else float(np.sum(np.asarray(q, dtype=np.float64) ** 2))
+    return float(lib().se_error_estimate(int(P), float(L), float(xi), Q, _mode(mode)))
+
+
 def derive(M: int, P: int, L: float, xi: float, m: float) -> Params:
     cfg = _lib.se_config(M=M, P=P, L=L, xi=xi, m=m, mode=0, precision=0, max_particles=0)
     out = [C.c_double() for _ in range(5)]
@@ -76,7 +94,9 @@ class SpectralEwald:
     ``max_particles`` particles (se_plan_create)."""
 
     def __init__(self, M: int, P: int, L: float = 1.0, xi: float = 8.0, m: float | None = None,
-                 mode="potential", precision="fp64", max_particles: int = 0):
+                 mode="potential", precision="fp64", max_particles: int = 0, path=None):
+        """path: None (the default kernels), "tune" (timed choice,
+        se_plan_create_ex with SE_PATH_TUNE) or SE_PATH_* bits."""
         self.M, self.P, self.L, self.xi = int(M), int(P), float(L), float(xi)
         self.m = float(default_m(P) if m is None else m)
         self.mode = _mode(mode)
@@ -86,12 +106,22 @@ class SpectralEwald:
                                   mode=self.mode, precision=self.precision,
                                   max_particles=self.max_particles)
         self._plan = C.c_void_p()
-        check(lib().se_plan_create(C.byref(self._plan), C.byref(self.cfg)), "se_plan_create")
+        if path is None:
+            check(lib().se_plan_create(C.byref(self._plan), C.byref(self.cfg)), "se_plan_create")
+        else:
+            code = _lib.SE_PATH_TUNE if path == "tune" else int(path)
+            check(lib().se_plan_create_ex(C.byref(self._plan), C.byref(self.cfg), code),
+                  "se_plan_create_ex")
         self.params = derive(self.M, self.P, self.L, self.xi, self.m)
 
     @property
     def out_width(self) -> int:
         return 3 if self.mode == SE_FORCE else 1
+
+    @property
+    def path(self) -> int:
+        """The kernel path this plan runs (SE_PATH_* bits)."""
+        return int(lib().se_plan_path(self._plan))
 
     def device_bytes(self) -> int:
         return int(lib().se_plan_device_bytes(C.byref(self.cfg)))

@@ -318,3 +318,19 @@ def test_nonfinite_position_reported(S):
     x[1] = 0.2
     out = se.solve_host(x, np.ones(4))
     assert np.isfinite(out).all()
+
+
+@pytest.mark.parametrize("eps", [1e-5, 1e-8, 1e-11])
+def test_chosen_params_reach_the_target(S, eps):
+    """se_choose_params' P and M give an absolute RMS error vs the direct
+    k-space sum within a small factor of the target (the estimate is the
+    reference's own, SE_init_params)."""
+    import oracle as O
+    g = load_golden("c1.npz")
+    x, q = g["x"], g["q"]
+    M, P, m = S.choose_params(eps, 1.0, 8.0, q, "potential")
+    se = S.SpectralEwald(M, P, 1.0, 8.0, m, "potential", "fp64", len(q))
+    phi = host(se.solve(cuda(x), cuda(q)))
+    err = O.abs_rms(phi, g["phi_direct"])
+    assert err < 10 * eps, (M, P, err)
+    se.close()
