@@ -93,7 +93,8 @@ int se_plan_destroy(se_plan plan);
  * plan runs.  SE_PATH_TILE_SPREAD and SE_PATH_PAIR_INTERP need M a multiple
  * of 16, M >= 32 and P <= 16; SE_PATH_RUNTIME_P turns off the interpolation
  * kernels specialised for P = 8, 12, 16 (21).  SE_PATH_DEFAULT is what
- * se_plan_create does (both tile kernels where they apply); SE_PATH_TUNE times
+ * se_plan_create does (the tile spread where it applies, the pair
+ * interpolation there too from P = 8 on); SE_PATH_TUNE times
  * every valid path on the plan's configuration (synthetic uniform particles,
  * N = max_particles, at most 2^20) and keeps the fastest, remembered per
  * (M, P, mode, precision, power-of-two class of N) for the process and, with

@@ -46,10 +46,14 @@ constexpr int PATH_TILE_SPREAD = 1;    // k_spread2 (else k_spread)
 constexpr int PATH_PAIR_INTERP = 2;    // k_interp2 (else k_interp / k_interp_global)
 constexpr int PATH_RUNTIME_P = 4;      // interpolation without the P-unrolled variants
 
-// The default path: the tile-aligned kernels wherever they apply.
+// The default path: the tile-aligned spread wherever it applies, and the
+// window-pair interpolation from P = 8 on (for shorter stencils its
+// per-particle set-up and z-pair padding cost more than they save: the timed
+// choice picks the general interpolation there on B200).
 __host__ __device__ inline int default_path(int M, int P)
 {
-    return spread2_eligible(M, P) ? PATH_TILE_SPREAD | PATH_PAIR_INTERP : 0;
+    if (!spread2_eligible(M, P)) return 0;
+    return PATH_TILE_SPREAD | (P >= 8 ? PATH_PAIR_INTERP : 0);
 }
 
 constexpr int MAX_SEG = 96;               // bin segments reaching one tile

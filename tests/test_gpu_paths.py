@@ -50,6 +50,7 @@ def test_paths_the_configuration_does_not_allow(env):
     se = S.SpectralEwald(24, 8, 1.0, 6.0, None, "force", "fp32", 100, path=4)
     assert se.path == 4
     assert S.SpectralEwald(32, 8, 1.0, 6.0, None, "force", "fp32", 100).path == 3
+    assert S.SpectralEwald(32, 6, 1.0, 6.0, None, "force", "fp32", 100).path == 1
     assert S.SpectralEwald(24, 8, 1.0, 6.0, None, "force", "fp32", 100).path == 0
 
 
