@@ -508,6 +508,7 @@ def main():
     # vs the FP64 direct k-space sum on the 1,000-particle subset
     accuracy = None
     fp64_ms = None
+    fft32 = None
     if rank == 0:
         se.solve(x, q, out)
         f32 = out.cpu().numpy()
@@ -529,7 +530,28 @@ def main():
             b.synchronize()
             t64.append(a.elapsed_time(b))
         fp64_ms = sum(t64) / len(t64)
-        del fl, o64
+        # the FP32-FFT mode on the same inputs, timed the same way
+        s3 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp32-fft32", N)
+        o3 = torch.empty(3 * N, dtype=torch.float64, device=dev)
+        s3.set_timing(True)
+        for _ in range(3):
+            s3.solve(x, q, o3)
+        t3, st3 = [], []
+        for k in range(10):
+            fl.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s3.solve(x, q, o3)
+            b.record(stream)
+            b.synchronize()
+            t3.append(a.elapsed_time(b))
+            st3.append(s3.stage_ms())
+        f3 = o3.cpu().numpy()
+        fft32 = {"ms_per_step": sum(t3) / len(t3), "value": N / (sum(t3) / len(t3) * 1e-3),
+                 "stage_ms": {k: sum(d[k] for d in st3) / len(st3) for k in st3[0]},
+                 "rel_rms_vs_fp64": O.rel_rms(f3, f64)}
+        s3.close()
+        del fl, o64, o3
         s64.close()
         accuracy = {"rel_rms_fp32_vs_fp64": O.rel_rms(f32, f64)}
         gpath = os.path.join(ROOT, "tests", "golden", "c2.npz")
@@ -540,6 +562,8 @@ def main():
             accuracy["rel_rms_vs_direct_1000"] = O.rel_rms(sub, g["force_direct"])
             sub64 = np.concatenate([f64[t + d * N] for d in range(3)])
             accuracy["rel_rms_fp64_vs_direct_1000"] = O.rel_rms(sub64, g["force_direct"])
+            sub3 = np.concatenate([f3[t + d * N] for d in range(3)])
+            fft32["rel_rms_vs_direct_1000"] = O.rel_rms(sub3, g["force_direct"])
 
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
     se.set_timing(True)
@@ -656,6 +680,7 @@ def main():
                 "ms_per_step": e2e},
         "gpu_launches": launches,
         "clocks": clk, "accuracy": accuracy, "wall_s_timed": wall,
+        "fp32_fft32": fft32,
         "fp64_plain": None if fp64_ms is None else {
             "ms_per_step": fp64_ms, "fp32_speedup": fp64_ms / ms,
             "note": "the FP64 path on the same inputs, same timing (5 steps, L2 flushed)"},

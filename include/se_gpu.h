@@ -50,7 +50,11 @@ enum {
 };
 
 enum { SE_POTENTIAL = 0, SE_FORCE = 1 };
-enum { SE_FP64 = 0, SE_FP32 = 1 };
+/* Precision of a plan or batch.  SE_FP64: every step in FP64.  SE_FP32:
+ * spread and interpolation in FP32 (compensated sums), FFTs and Z(k) in FP64.
+ * SE_FP32_FFT32: as SE_FP32 with the FFTs in FP32 as well (Z(k) still
+ * computed in FP64 and applied to the FP32 half spectrum). */
+enum { SE_FP64 = 0, SE_FP32 = 1, SE_FP32_FFT32 = 2 };
 
 typedef struct {
     int M;              /* grid points per dimension (cubic grid)              */
@@ -59,7 +63,7 @@ typedef struct {
     double xi;          /* Ewald parameter                                    */
     double m;           /* Gaussian shape factor                              */
     int mode;           /* SE_POTENTIAL or SE_FORCE                           */
-    int precision;      /* SE_FP64 or SE_FP32                                 */
+    int precision;      /* SE_FP64, SE_FP32 or SE_FP32_FFT32                  */
     int max_particles;  /* capacity of the plan                               */
 } se_config;
 
@@ -258,7 +262,7 @@ int se_solve_system(se_plan plan, const se_system* sys, const double* x, const d
 
 typedef struct {
     int slots;          /* solves in flight at once, 1..64                     */
-    int precision;      /* SE_FP32 or SE_FP64 gridding                         */
+    int precision;      /* SE_FP32, SE_FP32_FFT32 or SE_FP64                   */
     size_t hbm_budget;  /* device bytes the server may hold (plans + staging)  */
     int max_queue;      /* queued requests before submit says SE_ERR_BUSY; 0: no limit */
 } se_server_config;

@@ -90,7 +90,7 @@ SE_WHERE_HOST, SE_WHERE_DEVICE = 0, 1
 SE_PATH_DEFAULT, SE_PATH_TUNE = -1, -2
 SE_PATH_TILE_SPREAD, SE_PATH_PAIR_INTERP, SE_PATH_RUNTIME_P = 1, 2, 4
 SE_POTENTIAL, SE_FORCE = 0, 1
-SE_FP64, SE_FP32 = 0, 1
+SE_FP64, SE_FP32, SE_FP32_FFT32 = 0, 1, 2
 
 _ERR_NAMES = {1: "CUDA error", 2: "invalid argument", 3: "unsupported", 4: "out of memory",
               5: "cuFFT error", 6: "non-finite position", 7: "queue full",

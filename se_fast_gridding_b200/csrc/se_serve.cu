@@ -387,7 +387,8 @@ extern "C" size_t se_server_request_bytes(const se_system* sys, int precision)
 extern "C" int se_server_create(se_server* out, const se_server_config* cfg)
 {
     if (!out || !cfg || cfg->slots < 1 || cfg->slots > MAX_SLOTS || cfg->max_queue < 0 ||
-        (cfg->precision != SE_FP32 && cfg->precision != SE_FP64) || cfg->hbm_budget == 0)
+        (cfg->precision != SE_FP32 && cfg->precision != SE_FP64 &&
+         cfg->precision != SE_FP32_FFT32) || cfg->hbm_budget == 0)
         return SE_ERR_INVALID;
     se_server s = new se_server_s();
     s->cfg = *cfg;

@@ -223,8 +223,46 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale(const SysDev* __restric
     }
 }
 
+// The same Z, computed in FP64, applied to an FP32 half spectrum.
+__global__ void __launch_bounds__(SCALE_THREADS) k_scale32(const SysDev* __restrict__ sys,
+                                                           float2* __restrict__ spec)
+{
+    const SysDev& S = sys[blockIdx.y];
+    const int M = S.M, Mh = M / 2 + 1;
+    const int n = M * M * Mh;
+    float2* sp = spec + S.spec_off;
+    const int e0 = blockIdx.x * (SCALE_THREADS * SCALE_ITEMS) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < SCALE_ITEMS; k++) {
+        const int e = e0 + k * SCALE_THREADS;
+        if (e >= n) break;
+        const int r = e / Mh, iz = e - r * Mh;
+        const int ix = r / M, iy = r - ix * M;
+        const double kx = kwave(ix, M, S.kfac), ky = kwave(iy, M, S.kfac),
+                     kz = kwave(iz, M, S.kfac);
+        const double K2 = (kz * kz + ky * ky) + kx * kx;
+        const double Z = (e == 0) ? 0.0 : exp(S.scalar * K2) / K2 * S.dnorm;
+        float2 v = sp[e];
+        v.x = (float)((double)v.x * Z);
+        v.y = (float)((double)v.y * Z);
+        sp[e] = v;
+    }
+}
+
 #include "se_interp.cuh"
 #include "se_interp2.cuh"
+
+// FP32 grid back to FP64 (the FP32-FFT path feeding the general interpolation
+// or a caller's FP64 grid).
+__global__ void k_grid_to_f64(const float2* __restrict__ in, double2* __restrict__ out,
+                              long long n2)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n2;
+         e += (long long)gridDim.x * blockDim.x) {
+        const float2 v = in[e];
+        out[e] = make_double2((double)v.x, (double)v.y);
+    }
+}
 
 // ---------------------------------------------------------------- energy --
 
@@ -301,6 +339,8 @@ struct se_batch_s {
     bool any_interp1 = false, any_interp2 = false;   // on k_interp(_global) / k_interp2
     bool runtime_p = false;                          // some system asks for runtime P
     float* grid32 = nullptr;  // FP32 copy of the grids, staged by k_interp2<float>
+    bool fft32 = false;       // SE_FP32_FFT32: FP32 FFTs on grid32 / spec32
+    float2* spec32 = nullptr;
     int i2_P = 0;             // largest P of the k_interp2 systems (0: none)
     bool i2_uniform = false;  // all k_interp2 systems have P == i2_P
     int i2_Ep = 0, i2_PL = 0; // k_interp2 window pitches
@@ -422,6 +462,8 @@ static int path_of(const se_system* sys, const int* paths, int i)
 static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nbins_out,
                           int* ntiles_out, const int* paths = nullptr)
 {
+    const bool fft32 = precision == SE_FP32_FFT32;
+    if (fft32) precision = SE_FP32;
     long long ntot = 0, nbins = 0, ntiles = 0, grid = 0, spec = 0;
     for (int i = 0; i < nsys; i++) {
         const int M = sys[i].M;
@@ -447,12 +489,12 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     }
     if (plain) b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
     if (rows) b += (size_t)ntot * 3 * 32 * (precision == SE_FP32 ? 4 : 8);
-    if (pair && precision == SE_FP32) b += (size_t)grid * 4;   // FP32 copy of the grids
+    if ((pair && precision == SE_FP32) || fft32) b += (size_t)grid * 4;   // FP32 grids
     b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
     b += (size_t)(nbins + 1) * 4;
-    b += (size_t)grid * 8 + (size_t)spec * 16;
+    b += (size_t)grid * 8 + (size_t)spec * (fft32 ? 8 : 16);
     // cuFFT work areas are about one spectrum more
-    b += (size_t)spec * 16;
+    b += (size_t)spec * (fft32 ? 8 : 16);
     b += (size_t)nsys * (sizeof(SysDev) + 12) + 4096;
     return b;
 }
@@ -477,7 +519,7 @@ static int batch_free(se_batch b)
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
                     b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows,
-                    b->grid32};
+                    b->grid32, b->spec32};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -580,8 +622,11 @@ static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
 static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision,
                         const int* paths = nullptr)
 {
-    if (!out || !systems || nsys < 1 || (precision != SE_FP64 && precision != SE_FP32))
+    if (!out || !systems || nsys < 1 ||
+        (precision != SE_FP64 && precision != SE_FP32 && precision != SE_FP32_FFT32))
         return SE_ERR_INVALID;
+    const bool fft32 = precision == SE_FP32_FFT32;
+    if (fft32) precision = SE_FP32;   // FP32 gridding; the FFTs in FP32 too
     for (int i = 0; i < nsys; i++) {
         if (!valid_system(systems[i])) return SE_ERR_INVALID;
         const int path = path_of(systems, paths, i);
@@ -593,6 +638,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     se_batch b = new se_batch_s();
     b->nsys = nsys;
     b->precision = precision;
+    b->fft32 = fft32;
     // grids grouped by M (batched FFT plans need contiguous equal sizes)
     std::vector<int> order(nsys);
     for (int i = 0; i < nsys; i++) order[i] = i;
@@ -691,8 +737,9 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     }
     if (need_fac) SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
     if (need_rows) SE_ALLOC(b->rows, nt * 3 * 32 * (precision == SE_FP32 ? 4 : 8));
-    if (b->any_interp2 && precision == SE_FP32)
-        SE_ALLOC(b->grid32, sizeof(float) * b->grid_elems);
+    if ((b->any_interp2 && precision == SE_FP32) || fft32)
+        SE_ALLOC(b->grid32, sizeof(float) * (b->grid_elems + 16));
+    if (fft32) SE_ALLOC(b->spec32, sizeof(float2) * b->spec_elems);
     if (b->any_interp2) {
         b->i2_uniform = true;
         for (int i = 0; i < nsys; i++) {
@@ -705,8 +752,8 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     }
     b->sort_bytes = sort_scratch_bytes(b->ntot, std::max(b->nbins, 1));
     SE_ALLOC(b->sort_scratch, b->sort_bytes);
-    SE_ALLOC(b->grid, sizeof(double) * b->grid_elems);
-    SE_ALLOC(b->spec, sizeof(double2) * b->spec_elems);
+    SE_ALLOC(b->grid, sizeof(double) * (b->grid_elems + 16));
+    if (!fft32) SE_ALLOC(b->spec, sizeof(double2) * b->spec_elems);
     SE_ALLOC(b->energy_partial, sizeof(double) * 1024);
     SE_ALLOC(b->err, sizeof(int));
 #undef SE_ALLOC
@@ -727,10 +774,10 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         int n[3] = {g.M, g.M, g.M};
         const int idist = g.M * g.M * g.M, odist = g.M * g.M * (g.M / 2 + 1);
         cufftResult r = cufftPlanMany(&g.fwd, 3, n, nullptr, 1, idist, nullptr, 1, odist,
-                                      CUFFT_D2Z, g.count);
+                                      fft32 ? CUFFT_R2C : CUFFT_D2Z, g.count);
         if (r == CUFFT_SUCCESS)
-            r = cufftPlanMany(&g.bwd, 3, n, nullptr, 1, odist, nullptr, 1, idist, CUFFT_Z2D,
-                              g.count);
+            r = cufftPlanMany(&g.bwd, 3, n, nullptr, 1, odist, nullptr, 1, idist,
+                              fft32 ? CUFFT_C2R : CUFFT_Z2D, g.count);
         if (r != CUFFT_SUCCESS) return fail(cufft_fail(r, "cufftPlanMany"));
     }
     {
@@ -811,8 +858,56 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
     return SE_OK;
 }
 
+// FP64 <-> FP32 copies of the batch's grids (pairs; the allocations carry
+// one spare element so an odd total is covered).
+static int grid_f64_to_f32(se_batch b, const double* grid, cudaStream_t st)
+{
+    const long long n2 = (b->grid_elems + 1) / 2;
+    k_grid_to_f32<<<std::min<long long>(4096, ceil_div(n2, 256)), 256, 0, st>>>(
+        reinterpret_cast<const double2*>(grid), reinterpret_cast<float2*>(b->grid32), n2);
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
+static int grid_f32_to_f64(se_batch b, double* grid, cudaStream_t st)
+{
+    const long long n2 = (b->grid_elems + 1) / 2;
+    k_grid_to_f64<<<std::min<long long>(4096, ceil_div(n2, 256)), 256, 0, st>>>(
+        reinterpret_cast<const float2*>(b->grid32), reinterpret_cast<double2*>(grid), n2);
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    return SE_OK;
+}
+
+// SE_FP32_FFT32: the grid to FP32, R2C, Z (computed in FP64) on the FP32
+// half spectrum, C2R; the result stays in grid32.
+static int run_kspace32(se_batch b, const double* grid, cudaStream_t st)
+{
+    SE_TRY(grid_f64_to_f32(b, grid, st));
+    for (auto& g : b->groups) {
+        SE_CUFFT(cufftSetStream(g.fwd, st));
+        SE_CUFFT(cufftExecR2C(g.fwd, b->grid32 + g.grid_off,
+                              reinterpret_cast<cufftComplex*>(b->spec32 + g.spec_off)));
+    }
+    int maxM = 0;
+    for (auto& g : b->groups) maxM = std::max(maxM, g.M);
+    const dim3 gs(ceil_div((long)maxM * maxM * (maxM / 2 + 1), SCALE_THREADS * SCALE_ITEMS),
+                  b->nsys);
+    k_scale32<<<gs, SCALE_THREADS, 0, st>>>(b->sys, b->spec32);
+    SE_CUDA(cudaGetLastError());
+    LAUNCHED(b);
+    for (auto& g : b->groups) {
+        SE_CUFFT(cufftSetStream(g.bwd, st));
+        SE_CUFFT(cufftExecC2R(g.bwd, reinterpret_cast<cufftComplex*>(b->spec32 + g.spec_off),
+                              b->grid32 + g.grid_off));
+    }
+    return SE_OK;
+}
+
 static int run_kspace(se_batch b, double* grid, cudaStream_t st)
 {
+    if (b->fft32) return run_kspace32(b, grid, st);
     for (auto& g : b->groups) {
         SE_CUFFT(cufftSetStream(g.fwd, st));
         SE_CUFFT(cufftExecD2Z(g.fwd, grid + g.grid_off,
@@ -899,25 +994,24 @@ static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, c
     return SE_OK;
 }
 
-static int run_interp(se_batch b, const double* grid, double* out, double* phi, cudaStream_t st)
+// grid32_ready: the FP32-FFT k-space step left the grids in grid32 (the FP64
+// `grid` is then rebuilt from it only for the general interpolation).
+static int run_interp(se_batch b, double* grid, double* out, double* phi, cudaStream_t st,
+                      bool grid32_ready = false)
 {
     if (b->ntot == 0) return SE_OK;
     // systems of whole 16^3 tiles with P <= 16: k_interp2 (FP32 path from an
     // FP32 copy of the grids); the others: k_interp / k_interp_global
     if (b->any_interp2) {
         if (b->precision == SE_FP32) {
-            const long long n = b->grid_elems;
-            k_grid_to_f32<<<std::min<long long>(4096, ceil_div(n / 2 + 1, 256)), 256, 0, st>>>(
-                reinterpret_cast<const double2*>(grid), reinterpret_cast<float2*>(b->grid32),
-                n / 2);
-            SE_CUDA(cudaGetLastError());
-            LAUNCHED(b);
+            if (!grid32_ready) SE_TRY(grid_f64_to_f32(b, grid, st));
             SE_TRY(launch_interp2<float>(b, b->grid32, out, phi, st));
         } else {
             SE_TRY(launch_interp2<double>(b, grid, out, phi, st));
         }
     }
     if (!b->any_interp1) return SE_OK;
+    if (grid32_ready) SE_TRY(grid_f32_to_f64(b, grid, st));
     if (b->staged_interp) {
         if (b->precision == SE_FP32) return launch_interp_staged<float>(b, grid, out, phi, st);
         return launch_interp_staged<double>(b, grid, out, phi, st);
@@ -955,7 +1049,7 @@ static int batch_solve_direct(se_batch b, const double* x, const double* q, doub
     SE_TRY(mark(2));
     SE_TRY(run_kspace(b, b->grid, st));
     SE_TRY(mark(3));
-    SE_TRY(run_interp(b, b->grid, out, phi, st));
+    SE_TRY(run_interp(b, b->grid, out, phi, st, b->fft32));
     SE_TRY(mark(4));
     return SE_OK;
 }
@@ -1308,7 +1402,8 @@ extern "C" int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path)
     if (!plan || !cfg || cfg->max_particles < 0) return SE_ERR_INVALID;
     if (path == SE_PATH_DEFAULT) return se_plan_create(plan, cfg);
     se_system s = sys_of(cfg, cfg->max_particles);
-    if (!valid_system(s) || (cfg->precision != SE_FP32 && cfg->precision != SE_FP64))
+    if (!valid_system(s) || (cfg->precision != SE_FP32 && cfg->precision != SE_FP64 &&
+                             cfg->precision != SE_FP32_FFT32))
         return SE_ERR_INVALID;
     if (path == SE_PATH_TUNE) SE_TRY(tune_path(cfg, &path));
     if (path < 0 || path > 7) return SE_ERR_INVALID;
@@ -1442,7 +1537,10 @@ extern "C" int se_spread(se_plan p, int N, const double* x, const double* q, dou
 extern "C" int se_kspace(se_plan p, double* grid, void* stream)
 {
     if (!p || !grid) return SE_ERR_INVALID;
-    return run_kspace(p->b, grid, as_stream(stream));
+    cudaStream_t st = as_stream(stream);
+    SE_TRY(run_kspace(p->b, grid, st));
+    if (p->b->fft32) SE_TRY(grid_f32_to_f64(p->b, grid, st));   // the caller's grid is FP64
+    return SE_OK;
 }
 
 extern "C" int se_interp(se_plan p, int N, const double* x, const double* q, const double* grid,
@@ -1462,7 +1560,9 @@ extern "C" int se_interp(se_plan p, int N, const double* x, const double* q, con
                                 cudaMemcpyDeviceToDevice, st));
         grid = p->b->grid;
     }
-    return run_interp(p->b, grid, out, phi_out, st);
+    // only read: run_interp writes its grid argument when the FP32-FFT step left
+    // the result in grid32, which is not the case here
+    return run_interp(p->b, const_cast<double*>(grid), out, phi_out, st);
 }
 
 extern "C" int se_energy(const double* phi, const double* q, int N, double* e, void* stream)

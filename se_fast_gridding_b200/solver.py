@@ -33,7 +33,9 @@ def _prec(p) -> int:
         return SE_FP64
     if p in (SE_FP32, "fp32", "float32", torch.float32):
         return SE_FP32
-    raise ValueError(f"precision {p!r}: expected 'fp64' or 'fp32'")
+    if p in (_lib.SE_FP32_FFT32, "fp32-fft32"):
+        return _lib.SE_FP32_FFT32
+    raise ValueError(f"precision {p!r}: expected 'fp64', 'fp32' or 'fp32-fft32'")
 
 
 def _stream(stream) -> C.c_void_p:

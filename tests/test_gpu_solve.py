@@ -334,3 +334,53 @@ def test_chosen_params_reach_the_target(S, eps):
     err = O.abs_rms(phi, g["phi_direct"])
     assert err < 10 * eps, (M, P, err)
     se.close()
+
+
+def test_fp32_fft32_mode(S, c2):
+    """SE_FP32_FFT32 (FP32 FFTs, Z in FP64): C2 within the FP32 bound of the
+    FP64 path and of the direct sum."""
+    import oracle as O
+    g, x, q = c2
+    N, m = len(q), O.c1_params(16)
+    t = g["targets"]
+    for mode, key in (("force", "force"), ("potential", "phi")):
+        s64 = S.SpectralEwald(128, 16, 1.0, 20.0, m, mode, "fp64", N)
+        s32 = S.SpectralEwald(128, 16, 1.0, 20.0, m, mode, "fp32-fft32", N)
+        o64 = host(s64.solve(cuda(x), cuda(q)))
+        o32 = host(s32.solve(cuda(x), cuda(q)))
+        assert rel(o32, o64) < FP32_TOL, (mode, rel(o32, o64))
+        w = 3 if mode == "force" else 1
+        sub = np.concatenate([o32[t + d * N] for d in range(w)])
+        assert rel(sub, g[f"{key}_direct"]) < FP32_TOL
+
+
+def test_fp32_fft32_batch_and_steps(S):
+    import oracle as O
+    systems, xs, qs = [], [], []
+    for i in range(4):
+        N = 700 + 400 * i
+        M = (32, 24)[i % 2]          # tile-aligned and general kernels together
+        L = 1.0 + 0.3 * i
+        systems.append(S.System(N=N, M=M, P=(8, 12)[i % 2], L=L, xi=8.0 / L,
+                                mode=("force", "potential")[i % 2]))
+        x, q = O.synthetic_system(N, L, seed=60 + i)
+        xs.append(x)
+        qs.append(q)
+    b = S.BatchSolver(systems, precision="fp32-fft32")
+    xb, qb = b.pack(xs, qs)
+    outs = b.split(b.solve(xb, qb))
+    for s, x, q, o in zip(systems, xs, qs, outs):
+        one = host(S.SpectralEwald(s.M, s.P, s.L, s.xi, None, s.mode, "fp32-fft32",
+                                   s.N).solve(cuda(x), cuda(q)))
+        np.testing.assert_array_equal(host(o), one)
+        ref = O.spectral_ewald(x, q, s.M, s.P, S.default_m(s.P), s.L, s.xi, s.mode)
+        assert rel(one, ref) < FP32_TOL
+    # the k-space step keeps the caller's FP64 grid contract
+    s = systems[0]
+    x, q = xs[0], qs[0]
+    p64 = S.SpectralEwald(s.M, s.P, s.L, s.xi, None, s.mode, "fp64", s.N)
+    p32 = S.SpectralEwald(s.M, s.P, s.L, s.xi, None, s.mode, "fp32-fft32", s.N)
+    g64 = p64.kspace(p64.spread(cuda(x), cuda(q)))
+    g32 = p32.kspace(p32.spread(cuda(x), cuda(q)))
+    assert g32.dtype == g64.dtype
+    assert rel(host(g32), host(g64)) < FP32_TOL
