@@ -1160,6 +1160,7 @@ struct se_plan_s {
     double* d_x = nullptr;
     double* d_q = nullptr;
     double* d_out = nullptr;
+    int* h_err = nullptr;    // pinned: the input-error flag read back by se_solve_host
 };
 
 using namespace se;
@@ -1430,6 +1431,7 @@ extern "C" int se_plan_destroy(se_plan p)
     if (p->d_x) cudaFree(p->d_x);
     if (p->d_q) cudaFree(p->d_q);
     if (p->d_out) cudaFree(p->d_out);
+    if (p->h_err) cudaFreeHost(p->h_err);
     delete p;
     return SE_OK;
 }
@@ -1503,16 +1505,16 @@ extern "C" int se_solve_host(se_plan p, int N, const double* xh, const double* q
         SE_CUDA(cudaMalloc(&p->d_x, sizeof(double) * 3 * std::max(cap, 1)));
         SE_CUDA(cudaMalloc(&p->d_q, sizeof(double) * std::max(cap, 1)));
         SE_CUDA(cudaMalloc(&p->d_out, sizeof(double) * outw * std::max(cap, 1)));
+        SE_CUDA(cudaMallocHost(&p->h_err, sizeof(int)));
     }
     SE_CUDA(cudaMemcpyAsync(p->d_x, xh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
     SE_CUDA(cudaMemcpyAsync(p->d_q, qh, sizeof(double) * N, cudaMemcpyHostToDevice, st));
     SE_TRY(plan_set_N(p, N, st));
     SE_TRY(batch_solve(p->b, p->d_x, p->d_q, p->d_out, nullptr, st));
     SE_CUDA(cudaMemcpyAsync(outh, p->d_out, sizeof(double) * outw * N, cudaMemcpyDeviceToHost, st));
+    SE_CUDA(cudaMemcpyAsync(p->h_err, p->b->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SE_CUDA(cudaStreamSynchronize(st));
-    int err = 0;
-    SE_CUDA(cudaMemcpy(&err, p->b->err, sizeof(int), cudaMemcpyDeviceToHost));
-    return err ? SE_ERR_INPUT : SE_OK;
+    return *p->h_err ? SE_ERR_INPUT : SE_OK;
 }
 
 extern "C" int se_spread(se_plan p, int N, const double* x, const double* q, double* grid,
