@@ -12,6 +12,9 @@ D2Z, scaling, Z2D, unfold + interpolation) of that system.
 Timing: W untimed steps, then K steps each timed with CUDA events on the
 solve's stream; a 256 MiB buffer is written between steps so every step
 starts with a cold L2 (the inputs, 3.2 MB, and grids, 50 MB, would fit in it).
+The solves replay their CUDA graph (se_plan_set_graph, the repeated-solve
+launch mode); `direct_launch_ms_per_step` times the same solves launched
+one kernel at a time.
 Under torchrun every rank solves its own replica (weak scaling); the time is
 the max over ranks.  `e2e` repeats the measurement through se_solve_host with
 pinned host buffers (H2D of x, q and D2H of the forces inside the timed
@@ -498,11 +501,16 @@ def main():
     N = w["N"]
     x_np, q_np = O.synthetic_system(N, w["L"], seed=w["seed"] + rank, charges=w["charges"])
     m = solver.default_m(w["P"])
+    # every solve runs on a side stream and replays its CUDA graph (the
+    # repeated-solve launch mode, se_plan_set_graph); the direct launches are
+    # timed beside it
+    torch.cuda.set_stream(torch.cuda.Stream(dev))
+    stream = torch.cuda.current_stream(dev)
     se = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], w["precision"], N)
+    se.set_graph(True)
     x = torch.tensor(x_np, device=dev)
     q = torch.tensor(q_np, device=dev)
     out = torch.empty(3 * N, dtype=torch.float64, device=dev)
-    stream = torch.cuda.current_stream(dev)
 
     # accuracy (rank 0, outside the timed region): FP32 vs the FP64 path and
     # vs the FP64 direct k-space sum on the 1,000-particle subset
@@ -513,6 +521,7 @@ def main():
         se.solve(x, q, out)
         f32 = out.cpu().numpy()
         s64 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp64", N)
+        s64.set_graph(True)
         f64 = s64.solve(x, q).cpu().numpy()
         # the plain FP64 path on the same inputs, timed the same way (the
         # FP32 path is measured against it)
@@ -532,6 +541,7 @@ def main():
         fp64_ms = sum(t64) / len(t64)
         # the FP32-FFT mode on the same inputs, timed the same way
         s3 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp32-fft32", N)
+        s3.set_graph(True)
         o3 = torch.empty(3 * N, dtype=torch.float64, device=dev)
         s3.set_timing(True)
         for _ in range(3):
@@ -603,6 +613,21 @@ def main():
     value = world * N / (ms * 1e-3)
     stage_avg = {k: sum(v) / len(v) for k, v in stage.items()}
 
+    # the same solves launched directly (no graph), for comparison
+    se.set_graph(False)
+    se.set_timing(False)
+    direct = []
+    for k in range(max(args.warmup, 1) + args.steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        se.solve(x, q, out)
+        b.record(stream)
+        b.synchronize()
+        if k >= max(args.warmup, 1):
+            direct.append(a.elapsed_time(b))
+    direct_ms = sum(direct) / len(direct)
+
     # end to end through the host-buffer entry point, pinned buffers
     xh = torch.tensor(x_np).pin_memory()
     qh = torch.tensor(q_np).pin_memory()
@@ -672,9 +697,11 @@ def main():
         "data": "synthetic (seeded uniform charges and positions, one replica per GPU)",
         "config": {"workload": workload_name(w), "N": N, "M": M, "P": P, "xi": w["xi"],
                    "L": w["L"], "precision": w["precision"], "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (256 MiB write)"},
+                   "l2": "flushed between steps (256 MiB write)",
+                   "launch": "CUDA graph replay on a side stream (se_plan_set_graph); "
+                             "e2e: se_solve_host"},
         "roofline": roofline, "roofline_fma": roofline_fma,
-        "stage_ms": stage_avg, "cpu_baseline": cpu,
+        "stage_ms": stage_avg, "direct_launch_ms_per_step": direct_ms, "cpu_baseline": cpu,
         "e2e": {"value": world * N / (e2e * 1e-3), "unit": "particles/s",
                 "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 3 * N * 8,
                 "ms_per_step": e2e},

@@ -121,7 +121,11 @@ int se_plan_path(se_plan plan);
 int se_solve(se_plan plan, int N, const double* x, const double* q, double* out,
              double* phi_out, void* stream);
 
-/* The same through host buffers: copies in, solves, copies out, waits. */
+/* The same through host buffers: copies in, solves, copies out, waits (the
+ * drop-in for spectral_ewald(), which returns the result).  It runs after the
+ * work already queued on `stream`, on the plan's own stream, and replays the
+ * solve from a CUDA graph from its second call with the same N on (whatever
+ * se_plan_set_graph says: the device buffers are the plan's own). */
 int se_solve_host(se_plan plan, int N, const double* x_host, const double* q_host,
                   double* out_host, void* stream);
 
@@ -157,7 +161,7 @@ int se_plan_stage_ms(se_plan plan, float ms[4]);
  * (L, xi, m via se_solve_system) may change between replays.  Solves on the
  * legacy default stream always run directly.  Results are identical either
  * way. */
-int se_plan_set_graph(se_plan plan, int on);
+int se_plan_set_graph(se_plan plan, int on);   /* the device-buffer entry points */
 
 /* ------------------------------------------------- real space and self -- */
 /* The other two parts of the Ewald sum, for a cubic box of edge L (device

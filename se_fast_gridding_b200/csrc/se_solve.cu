@@ -311,6 +311,16 @@ struct FftGroup {
     cufftHandle fwd, bwd;
 };
 
+// A captured solve and the arguments it was captured with.
+struct GraphSlot {
+    cudaGraphExec_t exec = nullptr;
+    const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t stream = nullptr;
+    int ntot = -1, launches = 0;
+    bool timing = false;
+    bool warm = false;   // the first solve with these arguments ran directly
+};
+
 }  // namespace se
 
 struct se_batch_s {
@@ -360,15 +370,13 @@ struct se_batch_s {
     // per-stage CUDA events (prepare+sort, spread, k-space, interp)
     bool timing = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    // CUDA graph of one solve (se_*_set_graph): captured on the second solve
-    // with the same buffers, stream and particle count, replayed after that
+    // CUDA graphs of one solve: captured on the second solve with the same
+    // buffers, stream and particle count, replayed after that.  Slot 0
+    // serves the device-pointer entry points when se_*_set_graph turned it
+    // on; slot 1 the host-buffer entry point, which owns its buffers and
+    // stream and always replays.
     bool graph_on = false;
-    bool graph_warm = false;
-    cudaGraphExec_t gexec = nullptr;
-    const void* gkey[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaStream_t gstream = nullptr;
-    int gntot = -1, glaunches = 0;
-    bool gtiming = false;
+    se::GraphSlot gslot[2];
 };
 
 namespace se {
@@ -499,11 +507,16 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     return b;
 }
 
+static void graph_drop(GraphSlot& g)
+{
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    g.warm = false;
+}
+
 static void graph_drop(se_batch b)
 {
-    if (b->gexec) cudaGraphExecDestroy(b->gexec);
-    b->gexec = nullptr;
-    b->graph_warm = false;
+    for (auto& g : b->gslot) graph_drop(g);
 }
 
 static int batch_free(se_batch b)
@@ -1037,8 +1050,14 @@ static int batch_solve_direct(se_batch b, const double* x, const double* q, doub
 {
     b->launches = b->pending_launches;
     b->pending_launches = 0;
+    // stage events; inside a capture they become the graph's event-record
+    // nodes (external records), so replays time the stages too
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (b->timing) SE_CUDA(cudaStreamIsCapturing(st, &cs));
+    const unsigned rec_flags =
+        cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
     auto mark = [&](int i) -> int {
-        if (b->timing) SE_CUDA(cudaEventRecord(b->ev[i], st));
+        if (b->timing) SE_CUDA(cudaEventRecordWithFlags(b->ev[i], st, rec_flags));
         return SE_OK;
     };
     SE_CUDA(cudaMemsetAsync(b->err, 0, sizeof(int), st));
@@ -1054,61 +1073,62 @@ static int batch_solve_direct(se_batch b, const double* x, const double* q, doub
     return SE_OK;
 }
 
-// A solve through the batch's CUDA graph when graphs are on: the launch
-// sequence of a solve depends only on the buffers, the stream and the
-// particle count (the systems' parameters are read from the device table),
-// so a graph captured once replays every later solve with the same ones.
-// The legacy default streams cannot be captured: solves there run directly.
+// A solve through a CUDA graph: the launch sequence of a solve depends only
+// on the buffers, the stream and the particle count (the systems' parameters
+// are read from the device table), so a graph captured once replays every
+// later solve with the same ones.  Slot 0 (the device-pointer entry points)
+// replays only when graphs are on; the legacy default streams cannot be
+// captured, and solves there run directly.
 static int batch_solve(se_batch b, const double* x, const double* q, double* out, double* phi,
-                       cudaStream_t st)
+                       cudaStream_t st, int slot = 0)
 {
     const bool capturable = st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread;
-    if (!b->graph_on || !capturable) return batch_solve_direct(b, x, q, out, phi, st);
-    const bool same = b->gstream == st && b->gkey[0] == x && b->gkey[1] == q &&
-                      b->gkey[2] == out && b->gkey[3] == phi && b->gntot == b->ntot &&
-                      b->gtiming == b->timing;
+    if ((slot == 0 && !b->graph_on) || !capturable) return batch_solve_direct(b, x, q, out, phi, st);
+    GraphSlot& g = b->gslot[slot];
+    const bool same = g.stream == st && g.key[0] == x && g.key[1] == q && g.key[2] == out &&
+                      g.key[3] == phi && g.ntot == b->ntot && g.timing == b->timing;
     if (!same) {
-        graph_drop(b);
-        b->gstream = st;
-        b->gkey[0] = x;
-        b->gkey[1] = q;
-        b->gkey[2] = out;
-        b->gkey[3] = phi;
-        b->gntot = b->ntot;
-        b->gtiming = b->timing;
+        graph_drop(g);
+        g.stream = st;
+        g.key[0] = x;
+        g.key[1] = q;
+        g.key[2] = out;
+        g.key[3] = phi;
+        g.ntot = b->ntot;
+        g.timing = b->timing;
     }
-    if (!b->gexec && !b->graph_warm) {   // first solve: direct (sets up kernel attributes)
-        b->graph_warm = true;
+    if (!g.exec && !g.warm) {   // first solve: direct (sets up kernel attributes)
+        g.warm = true;
         return batch_solve_direct(b, x, q, out, phi, st);
     }
     const int pending = b->pending_launches;
     b->pending_launches = 0;
-    if (!b->gexec) {
+    if (!g.exec) {
         SE_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const int r = batch_solve_direct(b, x, q, out, phi, st);
-        cudaGraph_t g = nullptr;
-        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        cudaGraph_t gr = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &gr);
         if (r != SE_OK) {
-            if (g) cudaGraphDestroy(g);
+            if (gr) cudaGraphDestroy(gr);
             return r;
         }
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
-        const cudaError_t ei = cudaGraphInstantiate(&b->gexec, g, 0);
-        cudaGraphDestroy(g);
+        const cudaError_t ei = cudaGraphInstantiate(&g.exec, gr, 0);
+        cudaGraphDestroy(gr);
         if (ei != cudaSuccess) {
-            b->gexec = nullptr;
+            g.exec = nullptr;
             return cuda_fail(ei, "cudaGraphInstantiate", __FILE__, __LINE__);
         }
-        b->glaunches = b->launches;
+        g.launches = b->launches;
     }
-    SE_CUDA(cudaGraphLaunch(b->gexec, st));
-    b->launches = pending + b->glaunches;
+    SE_CUDA(cudaGraphLaunch(g.exec, st));
+    b->launches = pending + g.launches;
     return SE_OK;
 }
 
 static int set_graph(se_batch b, int on)
 {
-    if (!on) graph_drop(b);
+    if (!on) graph_drop(b->gslot[0]);
     b->graph_on = on != 0;
     return SE_OK;
 }
@@ -1154,13 +1174,14 @@ __global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters, float 
 struct se_plan_s {
     se_config cfg;
     se_batch b = nullptr;
-    double* h_x = nullptr;   // pinned staging for se_solve_host
-    double* h_q = nullptr;
-    double* h_out = nullptr;
+    // se_solve_host: device copies of the host buffers, the pinned input-error
+    // flag, and the stream (with its fence event) its graph is captured on
     double* d_x = nullptr;
     double* d_q = nullptr;
     double* d_out = nullptr;
-    int* h_err = nullptr;    // pinned: the input-error flag read back by se_solve_host
+    int* h_err = nullptr;
+    cudaStream_t hs = nullptr;
+    cudaEvent_t hev = nullptr;
 };
 
 using namespace se;
@@ -1425,9 +1446,8 @@ extern "C" int se_plan_destroy(se_plan p)
 {
     if (!p) return SE_OK;
     batch_free(p->b);
-    if (p->h_x) cudaFreeHost(p->h_x);
-    if (p->h_q) cudaFreeHost(p->h_q);
-    if (p->h_out) cudaFreeHost(p->h_out);
+    if (p->hs) cudaStreamDestroy(p->hs);
+    if (p->hev) cudaEventDestroy(p->hev);
     if (p->d_x) cudaFree(p->d_x);
     if (p->d_q) cudaFree(p->d_q);
     if (p->d_out) cudaFree(p->d_out);
@@ -1498,7 +1518,7 @@ extern "C" int se_solve_host(se_plan p, int N, const double* xh, const double* q
                              double* outh, void* stream)
 {
     if (!p || (N > 0 && (!xh || !qh || !outh))) return SE_ERR_INVALID;
-    cudaStream_t st = as_stream(stream);
+    cudaStream_t user = as_stream(stream);
     const int cap = p->cfg.max_particles;
     const int outw = p->cfg.mode == SE_FORCE ? 3 : 1;
     if (!p->d_x) {
@@ -1506,11 +1526,20 @@ extern "C" int se_solve_host(se_plan p, int N, const double* xh, const double* q
         SE_CUDA(cudaMalloc(&p->d_q, sizeof(double) * std::max(cap, 1)));
         SE_CUDA(cudaMalloc(&p->d_out, sizeof(double) * outw * std::max(cap, 1)));
         SE_CUDA(cudaMallocHost(&p->h_err, sizeof(int)));
+        SE_CUDA(cudaStreamCreateWithFlags(&p->hs, cudaStreamNonBlocking));
+        SE_CUDA(cudaEventCreateWithFlags(&p->hev, cudaEventDisableTiming));
     }
+    // The call runs on the plan's own stream, after the work queued on the
+    // caller's stream so far, and returns when it is done: the solve between
+    // the copies replays the plan's host-entry graph (same device buffers and
+    // stream every call; captured anew when N changes).
+    cudaStream_t st = p->hs;
+    SE_CUDA(cudaEventRecord(p->hev, user));
+    SE_CUDA(cudaStreamWaitEvent(st, p->hev, 0));
     SE_CUDA(cudaMemcpyAsync(p->d_x, xh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
     SE_CUDA(cudaMemcpyAsync(p->d_q, qh, sizeof(double) * N, cudaMemcpyHostToDevice, st));
     SE_TRY(plan_set_N(p, N, st));
-    SE_TRY(batch_solve(p->b, p->d_x, p->d_q, p->d_out, nullptr, st));
+    SE_TRY(batch_solve(p->b, p->d_x, p->d_q, p->d_out, nullptr, st, 1));
     SE_CUDA(cudaMemcpyAsync(outh, p->d_out, sizeof(double) * outw * N, cudaMemcpyDeviceToHost, st));
     SE_CUDA(cudaMemcpyAsync(p->h_err, p->b->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SE_CUDA(cudaStreamSynchronize(st));

@@ -1,7 +1,8 @@
 """Repeated solves replayed from a CUDA graph (se_plan_set_graph,
-se_batch_set_graph) give exactly the direct solves' results: positions that
-change in place between steps, a new particle count (a new capture), new box
-parameters between replays, and batches."""
+se_batch_set_graph, and the host-buffer entry point's own graph) give exactly
+the direct solves' results: positions that change in place between steps, a
+new particle count (a new capture), new box parameters between replays, and
+batches."""
 import numpy as np
 import pytest
 
@@ -61,6 +62,12 @@ def test_graph_replay_equals_direct(env, prec, M, P):
                                                                                  stream=s)
             s.synchronize()
             np.testing.assert_array_equal(out.cpu().numpy(), ref.cpu().numpy())
+    # stage timing inside replays
+    g.set_timing(True)
+    for _ in range(3):
+        g.solve(x, q, out, stream=s)
+    ms = g.stage_ms()
+    assert all(v > 0 for v in ms.values()), ms
     g.close()
     d.close()
 
@@ -86,3 +93,39 @@ def test_batch_graph_equals_direct(env):
             np.testing.assert_array_equal(out.cpu().numpy(), ref.cpu().numpy())
     bg.close()
     bd.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "fp32-fft32"])
+def test_host_entry_replays_equal_device_solves(env, prec):
+    """se_solve_host captures its solve on the second call with a given N and
+    replays it after that: new host buffers and contents every call, pinned or
+    pageable, a caller stream or the default one, N changing back and forth,
+    and an input error reported from a replay."""
+    torch, S, W = env
+    from se_fast_gridding_b200 import _lib
+    N = 2500
+    se = S.SpectralEwald(32, 8, 1.0, 8.0, None, "force", prec, N)
+    ref = S.SpectralEwald(32, 8, 1.0, 8.0, None, "force", prec, N)
+    side = torch.cuda.Stream()
+    for step, n in enumerate([N, N, N, 1200, 1200, N, 1200, 1200]):
+        xs, qs = W.synthetic_system(n, 1.0, seed=300 + step, charges="uniform")
+        if step % 2:
+            xh, qh = torch.tensor(xs).pin_memory(), torch.tensor(qs).pin_memory()
+            oh = torch.empty(3 * n, dtype=torch.float64).pin_memory()
+            se.solve_host_ptr(n, xh.data_ptr(), qh.data_ptr(), oh.data_ptr(),
+                              stream=side if step % 4 == 1 else None)
+            got = oh.numpy()
+        else:
+            got = se.solve_host(xs, qs)
+        want = ref.solve(torch.tensor(xs, device="cuda"), torch.tensor(qs, device="cuda"))
+        np.testing.assert_array_equal(got, want.cpu().numpy())
+    bad = W.synthetic_system(1200, 1.0, seed=9)[0]
+    bad[5] = np.nan
+    for _ in range(3):   # direct, captured and replayed with this N: reported every time
+        with pytest.raises(_lib.SEError):
+            se.solve_host(bad, np.ones(1200))
+    xs, qs = W.synthetic_system(1200, 1.0, seed=10)
+    np.testing.assert_array_equal(se.solve_host(xs, qs), ref.solve(
+        torch.tensor(xs, device="cuda"), torch.tensor(qs, device="cuda")).cpu().numpy())
+    se.close()
+    ref.close()
