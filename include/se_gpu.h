@@ -112,7 +112,13 @@ int se_plan_destroy(se_plan plan);
 #define SE_PATH_TILE_SPREAD 1
 #define SE_PATH_PAIR_INTERP 2
 #define SE_PATH_RUNTIME_P 4
+/* Sort the particles with the general multi-pass radix sort rather than the
+ * three-kernel bin sort used where it fits (<= 8192 fine bins, <= 2^19
+ * particles); both give the same permutation, so the results are identical. */
+#define SE_PATH_RADIX_SORT 8
 int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path);
+/* The path the default choice gives a system of grid M and stencil P. */
+int se_default_path(int M, int P);
 /* The path a plan runs (SE_PATH_* bits). */
 int se_plan_path(se_plan plan);
 
@@ -228,6 +234,10 @@ typedef struct {
 typedef struct se_batch_s* se_batch;
 
 int se_batch_create(se_batch* batch, const se_system* systems, int nsys, int precision);
+/* The same with each system's kernel path (SE_PATH_* bits; NULL: the
+ * defaults, as se_batch_create). */
+int se_batch_create_ex(se_batch* batch, const se_system* systems, int nsys, int precision,
+                       const int* paths);
 int se_batch_destroy(se_batch batch);
 size_t se_batch_device_bytes(const se_system* systems, int nsys, int precision);
 /* x: concatenated per-system SoA blocks (3 N_s each), q: concatenated N_s,

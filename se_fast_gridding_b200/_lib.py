@@ -88,7 +88,7 @@ SE_OK, SE_ERR_CUDA, SE_ERR_INVALID, SE_ERR_UNSUPPORTED, SE_ERR_NOMEM, SE_ERR_CUF
     SE_ERR_INPUT, SE_ERR_BUSY, SE_ERR_TIMEOUT = range(9)
 SE_WHERE_HOST, SE_WHERE_DEVICE = 0, 1
 SE_PATH_DEFAULT, SE_PATH_TUNE = -1, -2
-SE_PATH_TILE_SPREAD, SE_PATH_PAIR_INTERP, SE_PATH_RUNTIME_P = 1, 2, 4
+SE_PATH_TILE_SPREAD, SE_PATH_PAIR_INTERP, SE_PATH_RUNTIME_P, SE_PATH_RADIX_SORT = 1, 2, 4, 8
 SE_POTENTIAL, SE_FORCE = 0, 1
 SE_FP64, SE_FP32, SE_FP32_FFT32 = 0, 1, 2
 
@@ -135,6 +135,9 @@ def lib() -> C.CDLL:
         "se_sort_scratch_bytes": (C.c_size_t, [C.c_int, C.c_int]),
         "se_counting_sort": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, C.c_size_t, _vp]),
         "se_batch_create": (C.c_int, [C.POINTER(_vp), C.POINTER(se_system), C.c_int, C.c_int]),
+        "se_default_path": (C.c_int, [C.c_int, C.c_int]),
+        "se_batch_create_ex": (C.c_int, [C.POINTER(_vp), C.POINTER(se_system), C.c_int, C.c_int,
+                                         C.POINTER(C.c_int)]),
         "se_batch_destroy": (C.c_int, [_vp]),
         "se_batch_device_bytes": (C.c_size_t, [C.POINTER(se_system), C.c_int, C.c_int]),
         "se_batch_solve": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),

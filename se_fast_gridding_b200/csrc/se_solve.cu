@@ -61,15 +61,15 @@ static int cufft_fail(cufftResult r, const char* what)
 
 // --------------------------------------------------------------- prepare --
 
-__global__ void k_prepare(const SysDev* __restrict__ sys, const int* __restrict__ part_prefix,
-                          int nsys, int ntot, const double* __restrict__ x,
-                          const double* __restrict__ q, int* __restrict__ key,
-                          double4* __restrict__ rec, int* __restrict__ gpk, int* err)
+// Particle n (of system S, batch index) as the solve uses it: the stencil's
+// first grid point per axis (wrapped into [0, M)), the offset t0 of the
+// position from its nearest (odd P) or lower (even P) grid point, the charge
+// times the spread constant, and the fine-bin key.  False for a NaN, infinite
+// or absurd position: the particle then carries zero charge at cell 0.
+__device__ __forceinline__ bool particle_of(const SysDev& S, const double* __restrict__ x,
+                                            const double* __restrict__ q, int n, double4& rec,
+                                            int& gpk, int& key)
 {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= ntot) return;
-    const int s = find_sys(part_prefix, nsys, n);
-    const SysDev& S = sys[s];
     const int i = n - S.part_off;
     const double* xs = x + 3LL * S.part_off;
     const bool odd = S.P & 1;
@@ -79,21 +79,37 @@ __global__ void k_prepare(const SysDev* __restrict__ sys, const int* __restrict_
     for (int a = 0; a < 3; a++) {
         const double xa = xs[i + (long long)a * S.N];
         const double u = xa / S.h;
-        if (!(fabs(u) < 1.0e9)) {   // NaN / Inf / absurd positions
+        if (!(fabs(u) < 1.0e9)) {
             ok = false;
             t0[a] = 0.0;
             g[a] = 0;
             continue;
         }
         const int cell = odd ? (int)round(u) : (int)floor(u);
-        t0[a] = xa - S.h * cell;
+        t0[a] = __fma_rn(-S.h, (double)cell, xa);   // one rounding, in every kernel
         g[a] = pmod(cell + S.lo, S.M);
     }
-    if (!ok) atomicOr(err, 1);
-    const double qw = ok ? q[S.part_off + i] * S.d : 0.0;
-    rec[n] = make_double4(t0[0], t0[1], t0[2], qw);
-    gpk[n] = pack_g(g[0], g[1], g[2]);
-    key[n] = S.bin_base + ((g[0] / FB) * S.nf[1] + g[1] / FB) * S.nf[2] + g[2] / FB;
+    const double qw = ok ? q[n] * S.d : 0.0;
+    rec = make_double4(t0[0], t0[1], t0[2], qw);
+    gpk = pack_g(g[0], g[1], g[2]);
+    key = S.bin_base + ((g[0] / FB) * S.nf[1] + g[1] / FB) * S.nf[2] + g[2] / FB;
+    return ok;
+}
+
+__global__ void k_prepare(const SysDev* __restrict__ sys, const int* __restrict__ part_prefix,
+                          int nsys, int ntot, const double* __restrict__ x,
+                          const double* __restrict__ q, int* __restrict__ key,
+                          double4* __restrict__ rec, int* __restrict__ gpk, int* err)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ntot) return;
+    const SysDev& S = sys[find_sys(part_prefix, nsys, n)];
+    double4 r;
+    int g, k;
+    if (!particle_of(S, x, q, n, r, g, k)) atomicOr(err, 1);
+    rec[n] = r;
+    gpk[n] = g;
+    key[n] = k;
 }
 
 __global__ void k_gather(int ntot, const int* __restrict__ perm, const double4* __restrict__ rec,
@@ -106,6 +122,20 @@ __global__ void k_gather(int ntot, const int* __restrict__ perm, const double4* 
     srec[s] = rec[j];
     sg[s] = gpk[j];
 }
+
+// The recurrence's first factor v0 = exp(-c u0^2) and ratio
+// r0 = exp(2 c h u0 - c h^2), u0 = t0 - lo h, each operation rounded as
+// written (no contraction), so every kernel that builds factors gets the
+// same bits.
+__device__ __forceinline__ void factor_start(const SysDev& S, double t0, double& v, double& r)
+{
+    const double u0 = __dsub_rn(t0, __dmul_rn(S.lo, S.h));
+    v = exp(-__dmul_rn(__dmul_rn(S.c, u0), u0));
+    const double ch = __dmul_rn(S.c, S.h);
+    r = exp(__dsub_rn(__dmul_rn(__dmul_rn(2.0, ch), u0), __dmul_rn(ch, S.h)));
+}
+
+#include "se_binsort.cuh"
 
 // ------------------------------------------------------- factor rows -----
 
@@ -139,9 +169,8 @@ __global__ void __launch_bounds__(factors_threads<T>()) k_factors(
         const SysDev& S = sys[find_sys(part_prefix, nsys, sperm[s])];
         const double4 rc = srec[s];
         const double t0 = a == 0 ? rc.x : (a == 1 ? rc.y : rc.z);
-        const double u0 = t0 - S.lo * S.h;
-        double v = exp(-S.c * u0 * u0);
-        double r = exp(2.0 * S.c * S.h * u0 - S.c * S.h * S.h);
+        double v, r;
+        factor_start(S, t0, v, r);
         const int tiled = S.path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP);
         if (tiled) {
             staged = true;
@@ -357,6 +386,7 @@ struct se_batch_s {
     size_t i2_smem = 0;
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
+    bool bsort = false;   // the three-kernel bin sort (se_binsort.cuh) fits
     double* grid = nullptr;
     double2* spec = nullptr;
     double* energy_partial = nullptr;
@@ -498,7 +528,8 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     if (plain) b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
     if (rows) b += (size_t)ntot * 3 * 32 * (precision == SE_FP32 ? 4 : 8);
     if ((pair && precision == SE_FP32) || fft32) b += (size_t)grid * 4;   // FP32 grids
-    b += sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1));
+    b += std::max(sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1)),
+                  bsort_scratch_bytes((int)std::max<long long>(nbins, 1)));
     b += (size_t)(nbins + 1) * 4;
     b += (size_t)grid * 8 + (size_t)spec * (fft32 ? 8 : 16);
     // cuFFT work areas are about one spectrum more
@@ -643,7 +674,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     for (int i = 0; i < nsys; i++) {
         if (!valid_system(systems[i])) return SE_ERR_INVALID;
         const int path = path_of(systems, paths, i);
-        if (path < 0 || path > 7 ||
+        if (path < 0 || path > 15 ||
             ((path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP)) &&
              !spread2_eligible(systems[i].M, systems[i].P)))
             return SE_ERR_INVALID;
@@ -763,7 +794,11 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         interp2_pitch(b->i2_P, precision, &b->i2_Ep, &b->i2_PL);
         b->i2_smem = (size_t)(FB + b->i2_P - 1) * b->i2_PL * (precision == SE_FP32 ? 4 : 8);
     }
-    b->sort_bytes = sort_scratch_bytes(b->ntot, std::max(b->nbins, 1));
+    b->bsort = bsort_fits(b->ntot, b->nbins);
+    for (int i = 0; i < nsys; i++)
+        if (b->host_sys[i].path & PATH_RADIX_SORT) b->bsort = false;
+    b->sort_bytes = std::max(sort_scratch_bytes(b->ntot, std::max(b->nbins, 1)),
+                             b->bsort ? bsort_scratch_bytes(b->nbins) : size_t(0));
     SE_ALLOC(b->sort_scratch, b->sort_bytes);
     SE_ALLOC(b->grid, sizeof(double) * (b->grid_elems + 16));
     if (!fft32) SE_ALLOC(b->spec, sizeof(double2) * b->spec_elems);
@@ -821,8 +856,30 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
 
 static int run_factors(se_batch b, cudaStream_t st);
 
+static int run_bin_sort(se_batch b, const double* x, const double* q, cudaStream_t st)
+{
+    const int nk = b->nbins, chunk = bsort_chunk(b->ntot);
+    const int nch = ceil_div(b->ntot, chunk);
+    int* H = static_cast<int*>(b->sort_scratch);
+    int* T = H + (size_t)BSORT_MAX_CHUNKS * nk;
+    k_bsort_count<<<nch, BSORT_THREADS, sizeof(int) * nk, st>>>(
+        b->sys, b->d_part_prefix, b->nsys, b->ntot, x, q, chunk, nk, b->key, H, b->err);
+    SE_CUDA(cudaGetLastError());
+    k_bsort_columns<<<ceil_div(nk, 32), BSORT_COL_WARPS * 32, 0, st>>>(H, nch, nk, T);
+    SE_CUDA(cudaGetLastError());
+    const size_t smem = bsort_scatter_smem(b->ntot, nk);
+    SE_CUDA(raise_smem_limit((const void*)k_bsort_scatter, smem));
+    k_bsort_scatter<<<nch, BSORT_THREADS, smem, st>>>(b->sys, b->d_part_prefix, b->nsys,
+                                                      b->ntot, x, q, chunk, nk, b->key, H, T,
+                                                      b->boff, b->perm, b->srec, b->sg, b->err);
+    SE_CUDA(cudaGetLastError());
+    b->launches += 3;
+    return run_factors(b, st);
+}
+
 static int run_prepare_sort(se_batch b, const double* x, const double* q, cudaStream_t st)
 {
+    if (b->bsort && b->ntot > 0) return run_bin_sort(b, x, q, st);
     if (b->ntot > 0) {
         k_prepare<<<ceil_div(b->ntot, 256), 256, 0, st>>>(b->sys, b->d_part_prefix, b->nsys,
                                                           b->ntot, x, q, b->key, b->rec,
@@ -1428,7 +1485,7 @@ extern "C" int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path)
                              cfg->precision != SE_FP32_FFT32))
         return SE_ERR_INVALID;
     if (path == SE_PATH_TUNE) SE_TRY(tune_path(cfg, &path));
-    if (path < 0 || path > 7) return SE_ERR_INVALID;
+    if (path < 0 || path > 15) return SE_ERR_INVALID;
     se_plan p = new se_plan_s();
     p->cfg = *cfg;
     const int r = batch_create(&p->b, &s, 1, cfg->precision, &path);
@@ -1623,6 +1680,14 @@ extern "C" size_t se_batch_device_bytes(const se_system* systems, int nsys, int 
 extern "C" int se_batch_create(se_batch* b, const se_system* systems, int nsys, int precision)
 {
     return batch_create(b, systems, nsys, precision);
+}
+
+extern "C" int se_default_path(int M, int P) { return default_path(M, P); }
+
+extern "C" int se_batch_create_ex(se_batch* b, const se_system* systems, int nsys,
+                                  int precision, const int* paths)
+{
+    return batch_create(b, systems, nsys, precision, paths);
 }
 
 extern "C" int se_batch_destroy(se_batch b) { return batch_free(b); }

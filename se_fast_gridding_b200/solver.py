@@ -51,6 +51,11 @@ def _ptr(t: torch.Tensor | None) -> C.c_void_p:
     return C.c_void_p(t.data_ptr())
 
 
+def default_path(M: int, P: int) -> int:
+    """The SE_PATH_* bits the default kernel choice gives grid M, stencil P."""
+    return int(lib().se_default_path(int(M), int(P)))
+
+
 def default_m(P: int) -> float:
     """Gaussian shape factor m = 0.94 sqrt(pi P)."""
     return 0.94 * math.sqrt(PI * P)
@@ -244,14 +249,23 @@ class System:
 class BatchSolver:
     """Many independent systems in one set of launches (se_batch_*)."""
 
-    def __init__(self, systems: list[System], precision="fp32"):
+    def __init__(self, systems: list[System], precision="fp32", paths=None):
+        """paths: None (the default kernels) or one SE_PATH_* bit set per
+        system (se_batch_create_ex)."""
         self.systems = list(systems)
         self.precision = _prec(precision)
         arr = (_lib.se_system * len(self.systems))(*[s.c_struct() for s in self.systems])
         self._arr = arr
         self._b = C.c_void_p()
-        check(lib().se_batch_create(C.byref(self._b), arr, len(self.systems), self.precision),
-              "se_batch_create")
+        if paths is None:
+            check(lib().se_batch_create(C.byref(self._b), arr, len(self.systems),
+                                        self.precision), "se_batch_create")
+        else:
+            if len(paths) != len(self.systems):
+                raise ValueError("one path per system")
+            pa = (C.c_int * len(paths))(*[int(v) for v in paths])
+            check(lib().se_batch_create_ex(C.byref(self._b), arr, len(self.systems),
+                                           self.precision, pa), "se_batch_create_ex")
         self.part_off = np.concatenate([[0], np.cumsum([s.N for s in self.systems])])
         self.out_off = np.concatenate([[0], np.cumsum([s.N * s.out_width for s in self.systems])])
 

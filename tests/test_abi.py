@@ -115,3 +115,12 @@ def test_device_bytes_without_gpu(L):
                          max_particles=100_000)
     b = L.se_plan_device_bytes(C.byref(cfg))
     assert 128 ** 3 * 8 < b < 200 * 2 ** 20
+
+
+def test_default_path_without_gpu(L):
+    """Tile-aligned kernels for M a multiple of 16 (>= 32) and P <= 16, the
+    pair interpolation from P = 8 on."""
+    assert L.se_default_path(128, 16) == 3
+    assert L.se_default_path(64, 6) == 1
+    assert L.se_default_path(24, 8) == 0
+    assert L.se_default_path(128, 21) == 0
