@@ -10,36 +10,64 @@
 // most the home tile and the next one (periodically), and the row of tile
 // home + h is R[16h .. 16h + 15]: one aligned 64-byte copy, no wrap logic.
 //
-// One CTA of 4 warps owns one 16^3 tile.  It streams the particles of the
-// bin segments that reach the tile, keeps only those whose stencil really
-// meets it (in candidate order, through a ring queue: deterministic), and
-// takes them 64 at a time: their tile rows go to shared memory (the charge
-// folded into the x row), each warp lists the particles whose y rows meet its
-// 4 y planes, and each lane adds px[x] * (py[y] pz[z]) into 16 x 2 cells (all
-// 16 x of its (y, z) and (y, z + 1)).  Every cell is written once: no atomics
-// and a fixed order of summation.  FP32: fma.rn.f32x2 on the packed cells,
-// and after every 128 particles (two chunks) the FP32 sums are added into
-// FP64 in shared memory.
+// One CTA of 4 warps owns one 16^3 tile; warp w owns its y planes 4w..4w+3
+// (all 16 x and z), and after the CTA has listed the bin segments that reach
+// the tile the warps run independently, with no CTA barrier: each warp walks
+// the candidates of the segments in order, keeps the particles whose stencil
+// meets its planes (and the tile in x and z), and streams them in groups --
+// one particle per lane -- through two shared-memory stages that cp.async
+// fills from the factor rows while the warp works on the other: the x and z
+// tile rows, the warp's 4 y entries and the charge.  Each lane adds
+// px[x] * (q py[y] pz[z]) into 16 x 2 cells (all 16 x of its (y, z) and
+// (y, z + 1)).  Every cell belongs to one lane of one CTA: no atomics and a
+// fixed order of summation (the particles' candidate order).  FP32:
+// fma.rn.f32x2 on the packed cells, and after every 128 of the warp's
+// particles the FP32 sums are added into the FP64 grid in place (the first
+// time stored), which the lane alone reads and writes.
 
 constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
-constexpr int S2_CHUNK = 64;
-constexpr int S2_RING = 256;   // > S2_CHUNK + S2_THREADS
+constexpr int S2_LIST = 64;    // per-warp list ring: >= group - 1 + 32
 constexpr int S2_SEGS = 64;    // bin segments reaching a tile: <= 5 x 5 x 2 for P <= 16
+constexpr int S2_FOLD = 128;   // FP32 partial sums cover this many of a warp's particles
+
+// particles a warp stages at once: one per lane (FP32), half a warp (FP64)
+template <typename Acc>
+constexpr int s2_group() { return sizeof(Acc) == 4 ? 32 : 16; }
+
+template <typename Acc>
+struct Spread2Stage {
+    Acc px[s2_group<Acc>()][16];
+    Acc pz[s2_group<Acc>()][16];
+    Acc py[s2_group<Acc>()][4];
+    double q[s2_group<Acc>()];
+};
 
 template <typename Acc>
 struct Spread2Smem {
-    Acc px[S2_CHUNK][16];
-    Acc py[S2_CHUNK][16];
-    Acc pz[S2_CHUNK][16];
-    unsigned ymask[S2_CHUNK];
-    int list[S2_WARPS][S2_CHUNK];
-    int ring[S2_RING];
+    Spread2Stage<Acc> stage[S2_WARPS][2];
+    int2 list[S2_WARPS][S2_LIST];   // (particle, packed grid index)
     int seg_beg[S2_SEGS];
     int seg_pre[S2_SEGS];
     int wsum[S2_WARPS];
-    double fold[sizeof(Acc) == 4 ? 32 : 1][S2_THREADS];
 };
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // The 32 cells of one lane: 16 x for z and for z + 1.
 template <typename Acc>
@@ -66,22 +94,28 @@ struct Spread2Accum<float> {
             b[2 * m + 1] = ffma2(w.y, k1, b[2 * m + 1]);
         }
     }
-    // cell c: x = c >> 1, z + (c & 1)
-    __device__ __forceinline__ void fold(Spread2Smem<float>& sm, int t)
+    // cell (x, z + zz) at cell0 + x * plane + zz: the FP64 grid value plus
+    // this lane's FP32 partial sums (or the sums alone the first time)
+    __device__ __forceinline__ void fold(double* cell0, long long plane, bool first)
     {
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
-            const float2 u = f32x2_unpack(a[m]), v = f32x2_unpack(b[m]);
-            sm.fold[4 * m + 0][t] += (double)u.x;
-            sm.fold[4 * m + 1][t] += (double)v.x;
-            sm.fold[4 * m + 2][t] += (double)u.y;
-            sm.fold[4 * m + 3][t] += (double)v.y;
-            a[m] = b[m] = 0ull;
+        for (int h = 0; h < 2; h++) {
+            double2 old[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                old[k] = first ? make_double2(0.0, 0.0)
+                               : *reinterpret_cast<const double2*>(cell0 + (8 * h + k) * plane);
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) {
+                const int m = 4 * h + k / 2;
+                const float2 u = f32x2_unpack(a[m]), v = f32x2_unpack(b[m]);
+                *reinterpret_cast<double2*>(cell0 + (8 * h + k) * plane) =
+                    make_double2(old[k].x + (double)u.x, old[k].y + (double)v.x);
+                *reinterpret_cast<double2*>(cell0 + (8 * h + k + 1) * plane) =
+                    make_double2(old[k + 1].x + (double)u.y, old[k + 1].y + (double)v.y);
+                a[m] = b[m] = 0ull;
+            }
         }
-    }
-    __device__ __forceinline__ double2 result(const Spread2Smem<float>& sm, int t, int x) const
-    {
-        return make_double2(sm.fold[2 * x][t], sm.fold[2 * x + 1][t]);
     }
 };
 
@@ -105,10 +139,11 @@ struct Spread2Accum<double> {
             b[2 * m + 1] = fma(w.y, c1, b[2 * m + 1]);
         }
     }
-    __device__ __forceinline__ void fold(Spread2Smem<double>&, int) {}
-    __device__ __forceinline__ double2 result(const Spread2Smem<double>&, int, int x) const
+    __device__ __forceinline__ void store(double* cell0, long long plane) const
     {
-        return make_double2(a[x], b[x]);
+#pragma unroll
+        for (int x = 0; x < 16; x++)
+            *reinterpret_cast<double2*>(cell0 + x * plane) = make_double2(a[x], b[x]);
     }
 };
 
@@ -129,6 +164,8 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
     const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid)
 {
     constexpr bool FOLD = sizeof(Acc) == 4;
+    constexpr int G = s2_group<Acc>();
+    constexpr int V = 16 / sizeof(Acc);   // entries per 16-byte copy
     __shared__ __align__(16) Spread2Smem<Acc> sm;
 
     const int tile = blockIdx.x;
@@ -139,7 +176,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
     const int x0 = tix * 16, y0 = tiy * 16, z0 = tiz * 16;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int ly = warp * 4 + (lane >> 3), lz = (lane & 7) * 2;
+    const int ly = lane >> 3, lz = (lane & 7) * 2;
     const unsigned wbits = 0xFu << (warp * 4);
 
     // ---- the bin segments reaching this tile (at most 5 x 5 x 2) and their prefix
@@ -177,108 +214,99 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
         sm.seg_beg[t] = beg;
         sm.seg_pre[t] = before + incl - len;
     }
+    __syncthreads();   // the last CTA barrier: from here on the warps are independent
+
+    const unsigned pmask = (1u << P) - 1u;   // P <= 16
+    const unsigned lanes_before = (1u << lane) - 1u;
+    int2* list = sm.list[warp];
+    double* gs = grid + S.grid_off;
+    const long long plane = (long long)M * M;
+    double* cell0 = gs + (long long)x0 * plane + (long long)(y0 + warp * 4 + ly) * M + z0 + lz;
 
     Spread2Accum<Acc> acc;
     acc.zero();
-    if (FOLD)
-        for (int c = 0; c < 32; c++) sm.fold[c][t] = 0.0;
-    const unsigned pmask = (P >= 32) ? 0xffffffffu : ((1u << P) - 1u);
-
-    int head = 0, tail = 0, nfold = 0;
-    for (int cb = 0; cb < total; cb += S2_THREADS) {
-        __syncthreads();   // segment table ready; wsum free
-        // ---- candidates: keep the particles whose stencil meets the tile
-        const int pos = cb + t;
-        int part = -1;
-        if (pos < total) {
-            int lo = 0, hi = nseg - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sm.seg_pre[mid] <= pos) lo = mid;
-                else hi = mid - 1;
-            }
-            part = sm.seg_beg[lo] + (pos - sm.seg_pre[lo]);
-            const int pk = sg[part];
-            if (tile_half(g_of(pk, 0), tix, nt, P) < 0 || tile_half(g_of(pk, 1), tiy, nt, P) < 0 ||
-                tile_half(g_of(pk, 2), tiz, nt, P) < 0)
-                part = -1;
-        }
-        const unsigned keep = __ballot_sync(0xffffffffu, part >= 0);
-        if (lane == 0) sm.wsum[warp] = __popc(keep);
-        __syncthreads();
-        int wbefore = 0, added = 0;
-#pragma unroll
-        for (int w = 0; w < S2_WARPS; w++) {
-            const int v = sm.wsum[w];
-            wbefore += w < warp ? v : 0;
-            added += v;
-        }
-        if (part >= 0)
-            sm.ring[(tail + wbefore + __popc(keep & ((1u << lane) - 1u))) & (S2_RING - 1)] = part;
-        tail += added;
-        const bool last = cb + S2_THREADS >= total;
-
-        // ---- full chunks (and the remainder after the last candidates)
-        while (tail - head >= S2_CHUNK || (last && tail > head)) {
-            const int n = min(S2_CHUNK, tail - head);
-            __syncthreads();   // ring written; previous chunk's rows consumed
-            for (int it = t; it < 3 * n; it += S2_THREADS) {
-                const int a = it / n, p = it - a * n;
-                const int part = sm.ring[(head + p) & (S2_RING - 1)];
-                const int ga = g_of(sg[part], a);
-                const int h = tile_half(ga, a == 0 ? tix : (a == 1 ? tiy : tiz), nt, P);
-                if (a == 1) sm.ymask[p] = ((pmask << (ga & 15)) >> (16 * h)) & 0xFFFFu;
-                const Acc* src = rows + ((long long)part * 3 + a) * 32 + 16 * h;
-                Acc* dst = a == 0 ? sm.px[p] : (a == 1 ? sm.py[p] : sm.pz[p]);
-                if constexpr (sizeof(Acc) == 4) {
-                    const float4* s4 = reinterpret_cast<const float4*>(src);
-                    float4* d4 = reinterpret_cast<float4*>(dst);
-                    const float qw = a == 0 ? (float)srec[part].w : 1.0f;
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        float4 v = __ldg(s4 + k);
-                        v.x *= qw; v.y *= qw; v.z *= qw; v.w *= qw;
-                        d4[k] = v;
-                    }
-                } else {
-                    const double2* s2 = reinterpret_cast<const double2*>(src);
-                    double2* d2 = reinterpret_cast<double2*>(dst);
-                    const double qw = a == 0 ? srec[part].w : 1.0;
-#pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        double2 v = __ldg(s2 + k);
-                        v.x *= qw; v.y *= qw;
-                        d2[k] = v;
-                    }
+    int cpos = 0, head = 0, tail = 0, buf = 0, pending = 0, since_fold = 0;
+    bool written = false;
+    for (;;) {
+        // ---- list at least a group (or every remaining candidate), in order
+        while (tail - head < G && cpos < total) {
+            const int pos = cpos + lane;
+            int part = -1, pk = 0;
+            if (pos < total) {
+                int lo = 0, hi = nseg - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (sm.seg_pre[mid] <= pos) lo = mid;
+                    else hi = mid - 1;
                 }
+                part = sm.seg_beg[lo] + (pos - sm.seg_pre[lo]);
+                pk = sg[part];
+                const int gy = g_of(pk, 1);
+                const int hy = tile_half(gy, tiy, nt, P);
+                const bool meets = tile_half(g_of(pk, 0), tix, nt, P) >= 0 &&
+                                   tile_half(g_of(pk, 2), tiz, nt, P) >= 0 && hy >= 0 &&
+                                   ((((pmask << (gy & 15)) >> (16 * hy)) & 0xFFFFu) & wbits);
+                if (!meets) part = -1;
             }
-            __syncthreads();
-            // this warp's particles: y rows meeting its 4 y planes
-            int cnt = 0;
-            for (int base = 0; base < n; base += 32) {
-                const int q = base + lane;
-                const bool act = q < n && (sm.ymask[q] & wbits);
-                const unsigned bits = __ballot_sync(0xffffffffu, act);
-                if (act) sm.list[warp][cnt + __popc(bits & ((1u << lane) - 1u))] = q;
-                cnt += __popc(bits);
+            const unsigned keep = __ballot_sync(0xffffffffu, part >= 0);
+            if (part >= 0)
+                list[(tail + __popc(keep & lanes_before)) & (S2_LIST - 1)] = make_int2(part, pk);
+            tail += __popc(keep);
+            cpos += 32;
+        }
+        __syncwarp();   // list entries visible to the warp
+        // ---- stage the next group: lane l < n copies particle head + l
+        const int n = min(G, tail - head);
+        if (n > 0) {
+            Spread2Stage<Acc>& st = sm.stage[warp][buf];
+            if (lane < n) {
+                const int2 e = list[(head + lane) & (S2_LIST - 1)];
+                const int hx = tile_half(g_of(e.y, 0), tix, nt, P);
+                const int hy = tile_half(g_of(e.y, 1), tiy, nt, P);
+                const int hz = tile_half(g_of(e.y, 2), tiz, nt, P);
+                const Acc* r = rows + (long long)e.x * 96;
+#pragma unroll
+                for (int k = 0; k < 16; k += V) {
+                    cp_async16(&st.px[lane][k], r + 16 * hx + k);
+                    cp_async16(&st.pz[lane][k], r + 64 + 16 * hz + k);
+                }
+#pragma unroll
+                for (int k = 0; k < 4; k += V) cp_async16(&st.py[lane][k], r + 32 + 16 * hy + 4 * warp + k);
+                cp_async8(&st.q[lane], &srec[e.x].w);
             }
-            __syncwarp();
-            for (int i = 0; i < cnt; i++) {
-                const int p = sm.list[warp][i];
-                const Acc y = sm.py[p][ly];
-                const Acc c0 = y * sm.pz[p][lz], c1 = y * sm.pz[p][lz + 1];
-                acc.add(sm.px[p], c0, c1);
-            }
-            if (FOLD && (++nfold & 1) == 0) acc.fold(sm, t);
+            cp_async_commit();
             head += n;
         }
+        __syncwarp();   // the staged entries are read before the list refills over them
+        // ---- the previous group, while this one lands
+        if (pending > 0) {
+            if (n > 0) cp_async_wait<1>();
+            else cp_async_wait<0>();
+            __syncwarp();
+            const Spread2Stage<Acc>& st = sm.stage[warp][buf ^ 1];
+            for (int i = 0; i < pending; i++) {
+                const Acc y = st.py[i][ly] * (Acc)st.q[i];
+                acc.add(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
+            }
+            if constexpr (FOLD) {
+                since_fold += pending;
+                if (since_fold >= S2_FOLD) {
+                    acc.fold(cell0, plane, !written);
+                    written = true;
+                    since_fold = 0;
+                }
+            }
+            __syncwarp();   // the stage is read before it is refilled
+        }
+        if (n == 0) break;
+        pending = n;
+        buf ^= 1;
     }
 
-    if (FOLD) acc.fold(sm, t);
-    // ---- write the tile: 16 x of (y, z) and (y, z + 1) per lane
-    double* gs = grid + S.grid_off;
-    const long long row = ((long long)(y0 + ly)) * M + z0 + lz;
-#pragma unroll
-    for (int x = 0; x < 16; x++)
-        *reinterpret_cast<double2*>(gs + (long long)(x0 + x) * M * M + row) = acc.result(sm, t, x);
+    // ---- the lane's cells
+    if constexpr (FOLD) {
+        if (since_fold > 0 || !written) acc.fold(cell0, plane, !written);
+    } else {
+        acc.store(cell0, plane);
+    }
 }
