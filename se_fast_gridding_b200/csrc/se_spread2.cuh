@@ -226,20 +226,16 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
     Spread2Accum<Acc> acc;
     acc.zero();
     int cpos = 0, head = 0, tail = 0, buf = 0, pending = 0, since_fold = 0;
+    int seg = 0;   // the segment holding candidate cpos
     bool written = false;
     for (;;) {
         // ---- list at least a group (or every remaining candidate), in order
         while (tail - head < G && cpos < total) {
             const int pos = cpos + lane;
-            int part = -1, pk = 0;
+            int part = -1, pk = 0, sl = seg;   // this lane's segment, found forward
             if (pos < total) {
-                int lo = 0, hi = nseg - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (sm.seg_pre[mid] <= pos) lo = mid;
-                    else hi = mid - 1;
-                }
-                part = sm.seg_beg[lo] + (pos - sm.seg_pre[lo]);
+                while (sl + 1 < nseg && sm.seg_pre[sl + 1] <= pos) sl++;
+                part = sm.seg_beg[sl] + (pos - sm.seg_pre[sl]);
                 pk = sg[part];
                 const int gy = g_of(pk, 1);
                 const int hy = tile_half(gy, tiy, nt, P);
@@ -253,6 +249,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
                 list[(tail + __popc(keep & lanes_before)) & (S2_LIST - 1)] = make_int2(part, pk);
             tail += __popc(keep);
             cpos += 32;
+            seg = __reduce_max_sync(0xffffffffu, sl);
         }
         __syncwarp();   // list entries visible to the warp
         // ---- stage the next group: lane l < n copies particle head + l
@@ -284,6 +281,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
             else cp_async_wait<0>();
             __syncwarp();
             const Spread2Stage<Acc>& st = sm.stage[warp][buf ^ 1];
+#pragma unroll 2
             for (int i = 0; i < pending; i++) {
                 const Acc y = st.py[i][ly] * (Acc)st.q[i];
                 acc.add(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
