@@ -11,28 +11,19 @@ constexpr int SPREAD_THREADS = SPREAD_WARPS * 32;
 template <typename Acc>
 constexpr int spread_chunk() { return 64; }
 
-// Packed FP32 pairs (sm_100a): one fma.rn.f32x2 does two FP32 FMAs.
-__device__ __forceinline__ unsigned long long f32x2(float lo, float hi)
+// Packed FP32 pairs (sm_100a): one FFMA2 (__ffma2_rn) does two FP32 FMAs,
+// each rounded to nearest.
+__device__ __forceinline__ float2 f32x2(float lo, float hi) { return make_float2(lo, hi); }
+
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// The two packed pairs in 16 bytes of FP32 values.
+__device__ __forceinline__ void f32x2_split(const float4& v, float2& lo, float2& hi)
 {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
+    lo = make_float2(v.x, v.y);
+    hi = make_float2(v.z, v.w);
 }
 
-__device__ __forceinline__ float2 f32x2_unpack(unsigned long long v)
-{
-    float2 r;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
-    return r;
-}
-
-__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
-                                                    unsigned long long c)
-{
-    unsigned long long d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
 // The tile-aligned kernels (k_spread2, k_interp2 on tile-aligned factor rows)
 // apply when a system's grid is cut into whole 16^3 tiles and its stencil
 // fits two tiles.

@@ -34,18 +34,14 @@ struct Pair;
 
 template <>
 struct Pair<float> {
-    using V = unsigned long long;
+    using V = float2;
     __device__ __forceinline__ static V load(const float* p)
     {
         return *reinterpret_cast<const V*>(p);
     }
     __device__ __forceinline__ static V fma(V a, V b, V c) { return ffma2(a, b, c); }
-    __device__ __forceinline__ static float sum(V v)
-    {
-        const float2 f = f32x2_unpack(v);
-        return f.x + f.y;
-    }
-    __device__ __forceinline__ static V zero() { return 0ull; }
+    __device__ __forceinline__ static float sum(V v) { return v.x + v.y; }
+    __device__ __forceinline__ static V zero() { return make_float2(0.f, 0.f); }
 };
 
 template <>

@@ -77,31 +77,31 @@ struct SpreadAccum;
 
 template <>
 struct SpreadAccum<float> {
-    unsigned long long v[TX / 2];   // packed pairs (x = 2m, 2m + 1)
+    float2 v[TX / 2];   // packed pairs (x = 2m, 2m + 1)
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
-        for (int m = 0; m < TX / 2; m++) v[m] = 0ull;
+        for (int m = 0; m < TX / 2; m++) v[m] = make_float2(0.f, 0.f);
     }
     __device__ __forceinline__ void add(const float* px, float c)
     {
-        const unsigned long long cc = f32x2(c, c);
-        const ulonglong2* p2 = reinterpret_cast<const ulonglong2*>(px);
+        const float2 cc = f32x2(c, c);
+        const float4* p4 = reinterpret_cast<const float4*>(px);
 #pragma unroll
         for (int m = 0; m < TX / 4; m++) {
-            const ulonglong2 w = p2[m];
-            v[2 * m] = ffma2(w.x, cc, v[2 * m]);
-            v[2 * m + 1] = ffma2(w.y, cc, v[2 * m + 1]);
+            float2 lo, hi;
+            f32x2_split(p4[m], lo, hi);
+            v[2 * m] = ffma2(lo, cc, v[2 * m]);
+            v[2 * m + 1] = ffma2(hi, cc, v[2 * m + 1]);
         }
     }
     __device__ __forceinline__ void fold(SpreadSmem<float>& sm, int t)
     {
 #pragma unroll
         for (int m = 0; m < TX / 2; m++) {
-            const float2 f = f32x2_unpack(v[m]);
-            sm.fold[2 * m][t] += (double)f.x;
-            sm.fold[2 * m + 1][t] += (double)f.y;
-            v[m] = 0ull;
+            sm.fold[2 * m][t] += (double)v[m].x;
+            sm.fold[2 * m + 1][t] += (double)v[m].y;
+            v[m] = make_float2(0.f, 0.f);
         }
     }
     __device__ __forceinline__ double result(const SpreadSmem<float>& sm, int t, int x) const

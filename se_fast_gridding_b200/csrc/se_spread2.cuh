@@ -21,7 +21,7 @@
 // px[x] * (q py[y] pz[z]) into 16 x 2 cells (all 16 x of its (y, z) and
 // (y, z + 1)).  Every cell belongs to one lane of one CTA: no atomics and a
 // fixed order of summation (the particles' candidate order).  FP32:
-// fma.rn.f32x2 on the packed cells, and after every 128 of the warp's
+// packed FP32 pair FMAs on the cells, and after every 128 of the warp's
 // particles the FP32 sums are added into the FP64 grid in place (the first
 // time stored), which the lane alone reads and writes.
 
@@ -75,23 +75,24 @@ struct Spread2Accum;
 
 template <>
 struct Spread2Accum<float> {
-    unsigned long long a[8], b[8];   // packed x pairs for z and z + 1
+    float2 a[8], b[8];   // packed x pairs for z and z + 1
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
-        for (int m = 0; m < 8; m++) a[m] = b[m] = 0ull;
+        for (int m = 0; m < 8; m++) a[m] = b[m] = make_float2(0.f, 0.f);
     }
     __device__ __forceinline__ void add(const float* px, float c0, float c1)
     {
-        const unsigned long long k0 = f32x2(c0, c0), k1 = f32x2(c1, c1);
-        const ulonglong2* p2 = reinterpret_cast<const ulonglong2*>(px);
+        const float2 k0 = f32x2(c0, c0), k1 = f32x2(c1, c1);
+        const float4* p4 = reinterpret_cast<const float4*>(px);
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            const ulonglong2 w = p2[m];
-            a[2 * m] = ffma2(w.x, k0, a[2 * m]);
-            a[2 * m + 1] = ffma2(w.y, k0, a[2 * m + 1]);
-            b[2 * m] = ffma2(w.x, k1, b[2 * m]);
-            b[2 * m + 1] = ffma2(w.y, k1, b[2 * m + 1]);
+            float2 lo, hi;
+            f32x2_split(p4[m], lo, hi);
+            a[2 * m] = ffma2(lo, k0, a[2 * m]);
+            a[2 * m + 1] = ffma2(hi, k0, a[2 * m + 1]);
+            b[2 * m] = ffma2(lo, k1, b[2 * m]);
+            b[2 * m + 1] = ffma2(hi, k1, b[2 * m + 1]);
         }
     }
     // cell (x, z + zz) at cell0 + x * plane + zz: the FP64 grid value plus
@@ -108,12 +109,12 @@ struct Spread2Accum<float> {
 #pragma unroll
             for (int k = 0; k < 8; k += 2) {
                 const int m = 4 * h + k / 2;
-                const float2 u = f32x2_unpack(a[m]), v = f32x2_unpack(b[m]);
+                const float2 u = a[m], v = b[m];
                 *reinterpret_cast<double2*>(cell0 + (8 * h + k) * plane) =
                     make_double2(old[k].x + (double)u.x, old[k].y + (double)v.x);
                 *reinterpret_cast<double2*>(cell0 + (8 * h + k + 1) * plane) =
                     make_double2(old[k + 1].x + (double)u.y, old[k + 1].y + (double)v.y);
-                a[m] = b[m] = 0ull;
+                a[m] = b[m] = make_float2(0.f, 0.f);
             }
         }
     }
