@@ -62,8 +62,10 @@ struct Pair<double> {
 // z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
 __host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
 
-template <typename T, int PT>
-__global__ void __launch_bounds__(I2_WARPS * 32) k_interp2(
+// FORCE: the force weights and sums are computed (every system of a batch
+// with a FORCE system runs this variant; each stores what its mode asks).
+template <typename T, int PT, bool FORCE>
+__global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_interp2(
     const SysDev* __restrict__ sys, const int* __restrict__ bin_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const int* __restrict__ sperm, const T* __restrict__ rows, const int* __restrict__ boff,
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(I2_WARPS * 32) k_interp2(
     __syncthreads();
 
     Interp2Warp<T>& W = wsm[warp];
-    const bool force = S.mode == SE_FORCE;
+    constexpr bool force = FORCE;
     constexpr int NQ = PT ? PT / 2 + 1 : 9;   // z pairs a stencil spans (<= 9 for P <= 16)
     const int nq = P / 2 + 1;
     const bool JFIX = (32 % P) == 0;
@@ -206,8 +208,8 @@ __global__ void __launch_bounds__(I2_WARPS * 32) k_interp2(
             d_fz = warp_sum(d_fz);
         }
         if (lane == 0)
-            interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz, force, out,
-                         phi_out);
+            interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz,
+                         S.mode == SE_FORCE, out, phi_out);
         __syncwarp();
     }
 }

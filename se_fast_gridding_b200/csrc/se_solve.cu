@@ -1040,28 +1040,39 @@ static int run_factors(se_batch b, cudaStream_t st)
     return SE_OK;
 }
 
-template <typename T>
-static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, cudaStream_t st)
+template <typename T, bool FORCE>
+static int launch_interp2_mode(se_batch b, const T* grid, double* out, double* phi,
+                               cudaStream_t st)
 {
     const int P = b->i2_P;
     const bool u = b->i2_uniform && !b->runtime_p;
-    const void* fn = (u && P == 8)    ? (const void*)k_interp2<T, 8>
-                     : (u && P == 12) ? (const void*)k_interp2<T, 12>
-                     : (u && P == 16) ? (const void*)k_interp2<T, 16>
-                                      : (const void*)k_interp2<T, 0>;
+    const void* fn = (u && P == 8)    ? (const void*)k_interp2<T, 8, FORCE>
+                     : (u && P == 12) ? (const void*)k_interp2<T, 12, FORCE>
+                     : (u && P == 16) ? (const void*)k_interp2<T, 16, FORCE>
+                                      : (const void*)k_interp2<T, 0, FORCE>;
     SE_CUDA(raise_smem_limit(fn, b->i2_smem));
     const dim3 grd(std::max(b->nbins, 1)), blk(I2_WARPS * 32);
     const T* rows = static_cast<const T*>(b->rows);
 #define SE_I2ARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, rows, b->boff, grid, \
                   out, phi, b->i2_Ep, b->i2_PL
-    if (u && P == 8) k_interp2<T, 8><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
-    else if (u && P == 12) k_interp2<T, 12><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
-    else if (u && P == 16) k_interp2<T, 16><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
-    else k_interp2<T, 0><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    if (u && P == 8) k_interp2<T, 8, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    else if (u && P == 12) k_interp2<T, 12, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    else if (u && P == 16) k_interp2<T, 16, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+    else k_interp2<T, 0, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
 #undef SE_I2ARGS
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     return SE_OK;
+}
+
+template <typename T>
+static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, cudaStream_t st)
+{
+    bool any_force = false;
+    for (const auto& S : b->host_sys)
+        if ((S.path & PATH_PAIR_INTERP) && S.mode == SE_FORCE) any_force = true;
+    return any_force ? launch_interp2_mode<T, true>(b, grid, out, phi, st)
+                     : launch_interp2_mode<T, false>(b, grid, out, phi, st);
 }
 
 // grid32_ready: the FP32-FFT k-space step left the grids in grid32 (the FP64
