@@ -21,7 +21,7 @@
 // px[x] * (q py[y] pz[z]) into 16 x 2 cells (all 16 x of its (y, z) and
 // (y, z + 1)).  Every cell belongs to one lane of one CTA: no atomics and a
 // fixed order of summation (the particles' candidate order).  FP32:
-// packed FP32 pair FMAs on the cells, and after every 256 of the warp's
+// packed FP32 pair FMAs on the cells, and after every 512 of the warp's
 // particles the FP32 sums are added into the FP64 grid in place (the first
 // time stored), which the lane alone reads and writes.
 
@@ -29,7 +29,7 @@ constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
 constexpr int S2_LIST = 64;    // per-warp list ring: >= group - 1 + 32
 constexpr int S2_SEGS = 64;    // bin segments reaching a tile: <= 5 x 5 x 2 for P <= 16
-constexpr int S2_FOLD = 256;   // FP32 partial sums cover this many of a warp's particles
+constexpr int S2_FOLD = 512;   // FP32 partial sums cover this many of a warp's particles
 
 // particles a warp stages at once: one per lane (FP32), half a warp (FP64)
 template <typename Acc>
