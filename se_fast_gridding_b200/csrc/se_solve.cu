@@ -225,12 +225,14 @@ __device__ __forceinline__ double kwave(int i, int M, double kfac)
 // with K2 summed in the reference's order (its first FFT axis is our z).
 constexpr int SCALE_THREADS = 256, SCALE_ITEMS = 8;
 
-// Elements e = blockIdx.x * SCALE_THREADS * SCALE_ITEMS + ... of one
-// system's half spectrum [x][y][z <= M/2]; 32-bit index arithmetic.
+// Elements e = blockIdx.x * SCALE_THREADS * SCALE_ITEMS + ... of the half
+// spectrum [x][y][z <= M/2] of system order[first + blockIdx.y]; 32-bit
+// index arithmetic.
 __global__ void __launch_bounds__(SCALE_THREADS) k_scale(const SysDev* __restrict__ sys,
+                                                         const int* __restrict__ order, int first,
                                                          double2* __restrict__ spec)
 {
-    const SysDev& S = sys[blockIdx.y];
+    const SysDev& S = sys[order[first + blockIdx.y]];
     const int M = S.M, Mh = M / 2 + 1;
     const int n = M * M * Mh;
     double2* sp = spec + S.spec_off;
@@ -278,6 +280,7 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale32(const SysDev* __restr
     }
 }
 
+#include "se_fft.cuh"
 #include "se_interp.cuh"
 #include "se_interp2.cuh"
 
@@ -336,6 +339,8 @@ struct HostSys {
 
 struct FftGroup {
     int M, count;
+    int first;     // its systems are order[first .. first + count)
+    bool custom;   // the three-pass FFT (se_fft.cuh), else cuFFT
     long long grid_off, spec_off;
     cufftHandle fwd, bwd;
 };
@@ -387,6 +392,8 @@ struct se_batch_s {
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     bool bsort = false;   // the three-kernel bin sort (se_binsort.cuh) fits
+    int* d_order = nullptr;      // system indices grouped by M (the FFT groups)
+    double2* fft_tw = nullptr;   // W_128^k, k < 128, for the three-pass FFT
     double* grid = nullptr;
     double2* spec = nullptr;
     double* energy_partial = nullptr;
@@ -563,7 +570,7 @@ static int batch_free(se_batch b)
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
                     b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows,
-                    b->grid32, b->spec32};
+                    b->grid32, b->spec32, b->d_order, b->fft_tw};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -674,7 +681,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     for (int i = 0; i < nsys; i++) {
         if (!valid_system(systems[i])) return SE_ERR_INVALID;
         const int path = path_of(systems, paths, i);
-        if (path < 0 || path > 15 ||
+        if (path < 0 || path > 31 ||
             ((path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP)) &&
              !spread2_eligible(systems[i].M, systems[i].P)))
             return SE_ERR_INVALID;
@@ -698,6 +705,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
             FftGroup g{};
             g.M = M;
             g.count = 0;
+            g.first = k;
             g.grid_off = gcur;
             g.spec_off = scur;
             b->groups.push_back(g);
@@ -804,6 +812,8 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     if (!fft32) SE_ALLOC(b->spec, sizeof(double2) * b->spec_elems);
     SE_ALLOC(b->energy_partial, sizeof(double) * 1024);
     SE_ALLOC(b->err, sizeof(int));
+    SE_ALLOC(b->d_order, sizeof(int) * nsys);
+    SE_ALLOC(b->fft_tw, sizeof(double2) * 128);
 #undef SE_ALLOC
     cudaError_t e = cudaMemcpy(b->sys, b->host_sys.data(), sizeof(SysDev) * nsys,
                                cudaMemcpyHostToDevice);
@@ -817,8 +827,26 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         e = cudaMemcpy(b->d_bin_prefix, b->bin_prefix.data(), sizeof(int) * (nsys + 1),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(b->err, 0, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_order, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        // W_128^k = exp(-2 pi i k / 128), rounded once from long double
+        double2 tw[128];
+        const long double two_pi = 6.283185307179586476925286766559005768L;
+        for (int k = 0; k < 128; k++) {
+            const long double a = two_pi * (long double)k / 128.0L;
+            tw[k] = make_double2((double)cosl(a), (double)-sinl(a));
+        }
+        e = cudaMemcpy(b->fft_tw, tw, sizeof(tw), cudaMemcpyHostToDevice);
+    }
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemcpy", __FILE__, __LINE__));
+    // the three-pass FFT takes the FP64 transforms of M = 32, 64, 128
+    bool cufft_all = fft32;
+    for (int i = 0; i < nsys; i++)
+        if (b->host_sys[i].path & PATH_CUFFT) cufft_all = true;
+    for (auto& g : b->groups) g.custom = !cufft_all && (g.M == 32 || g.M == 64 || g.M == 128);
     for (auto& g : b->groups) {
+        if (g.custom) continue;
         int n[3] = {g.M, g.M, g.M};
         const int idist = g.M * g.M * g.M, odist = g.M * g.M * (g.M / 2 + 1);
         cufftResult r = cufftPlanMany(&g.fwd, 3, n, nullptr, 1, idist, nullptr, 1, odist,
@@ -846,6 +874,15 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     }
     if (b->staged_interp) {
         const cudaError_t a = raise_smem_limit(staged_interp_kernel(b), b->interp_smem);
+        if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
+    }
+    for (const auto& g : b->groups) {
+        if (!g.custom) continue;
+        cudaError_t a = cudaSuccess;
+        if (g.M == 128) {
+            a = raise_smem_limit((const void*)k_fft_zy<128>, fft_plane_smem<128>());
+            if (a == cudaSuccess) a = raise_smem_limit((const void*)k_ifft_yz<128>, fft_plane_smem<128>());
+        }
         if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
     }
     *out = b;
@@ -975,22 +1012,52 @@ static int run_kspace32(se_batch b, const double* grid, cudaStream_t st)
     return SE_OK;
 }
 
-static int run_kspace(se_batch b, double* grid, cudaStream_t st)
+// The three passes of se_fft.cuh for group g; grid32 (may be null) receives
+// the FP32 copy of the result beside the FP64 grid.
+template <int M>
+static int launch_fft3(se_batch b, const FftGroup& g, double* grid, float* grid32, cudaStream_t st)
 {
+    const unsigned planes = (unsigned)(g.count * M);
+    k_fft_zy<M><<<planes, FFT_THREADS, fft_plane_smem<M>(), st>>>(b->sys, b->d_order, g.first,
+                                                                  grid, b->spec, b->fft_tw);
+    SE_CUDA(cudaGetLastError());
+    k_fft_x_scale<M><<<(unsigned)(g.count * M * fft_x_blocks<M>()), FFT_X_THREADS, 0, st>>>(
+        b->sys, b->d_order, g.first, b->spec, b->fft_tw);
+    SE_CUDA(cudaGetLastError());
+    k_ifft_yz<M><<<planes, FFT_THREADS, fft_plane_smem<M>(), st>>>(
+        b->sys, b->d_order, g.first, b->spec, grid, grid32, b->fft_tw);
+    SE_CUDA(cudaGetLastError());
+    b->launches += 3;
+    return SE_OK;
+}
+
+// grid32_fresh (may be null): set when every group's result was also
+// written to the FP32 grids.
+static int run_kspace(se_batch b, double* grid, cudaStream_t st, bool* grid32_fresh = nullptr)
+{
+    if (grid32_fresh) *grid32_fresh = false;
     if (b->fft32) return run_kspace32(b, grid, st);
-    for (auto& g : b->groups) {
+    bool all_custom = true;
+    for (const auto& g : b->groups) all_custom = all_custom && g.custom;
+    float* g32 = (all_custom && b->grid32) ? b->grid32 : nullptr;
+    for (const auto& g : b->groups) {
+        if (!g.custom) continue;
+        // the kernels add each system's own grid offset to the batch's bases
+        if (g.M == 128) SE_TRY(launch_fft3<128>(b, g, grid, g32, st));
+        else if (g.M == 64) SE_TRY(launch_fft3<64>(b, g, grid, g32, st));
+        else SE_TRY(launch_fft3<32>(b, g, grid, g32, st));
+    }
+    if (grid32_fresh) *grid32_fresh = g32 != nullptr;
+    for (const auto& g : b->groups) {
+        if (g.custom) continue;
         SE_CUFFT(cufftSetStream(g.fwd, st));
         SE_CUFFT(cufftExecD2Z(g.fwd, grid + g.grid_off,
                               reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off)));
-    }
-    int maxM = 0;
-    for (auto& g : b->groups) maxM = std::max(maxM, g.M);
-    const dim3 gs(ceil_div((long)maxM * maxM * (maxM / 2 + 1), SCALE_THREADS * SCALE_ITEMS),
-                  b->nsys);
-    k_scale<<<gs, SCALE_THREADS, 0, st>>>(b->sys, b->spec);
-    SE_CUDA(cudaGetLastError());
-    LAUNCHED(b);
-    for (auto& g : b->groups) {
+        const dim3 gs(ceil_div((long)g.M * g.M * (g.M / 2 + 1), SCALE_THREADS * SCALE_ITEMS),
+                      g.count);
+        k_scale<<<gs, SCALE_THREADS, 0, st>>>(b->sys, b->d_order, g.first, b->spec);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
         SE_CUFFT(cufftSetStream(g.bwd, st));
         SE_CUFFT(cufftExecZ2D(g.bwd,
                               reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off),
@@ -1075,17 +1142,18 @@ static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, c
                      : launch_interp2_mode<T, false>(b, grid, out, phi, st);
 }
 
+// grid32_fresh: grid32 holds the FP32 copy of `grid` already.
 // grid32_ready: the FP32-FFT k-space step left the grids in grid32 (the FP64
 // `grid` is then rebuilt from it only for the general interpolation).
 static int run_interp(se_batch b, double* grid, double* out, double* phi, cudaStream_t st,
-                      bool grid32_ready = false)
+                      bool grid32_ready = false, bool grid32_fresh = false)
 {
     if (b->ntot == 0) return SE_OK;
     // systems of whole 16^3 tiles with P <= 16: k_interp2 (FP32 path from an
     // FP32 copy of the grids); the others: k_interp / k_interp_global
     if (b->any_interp2) {
         if (b->precision == SE_FP32) {
-            if (!grid32_ready) SE_TRY(grid_f64_to_f32(b, grid, st));
+            if (!grid32_ready && !grid32_fresh) SE_TRY(grid_f64_to_f32(b, grid, st));
             SE_TRY(launch_interp2<float>(b, b->grid32, out, phi, st));
         } else {
             SE_TRY(launch_interp2<double>(b, grid, out, phi, st));
@@ -1134,9 +1202,10 @@ static int batch_solve_direct(se_batch b, const double* x, const double* q, doub
     SE_TRY(mark(1));
     SE_TRY(run_spread(b, b->grid, st));
     SE_TRY(mark(2));
-    SE_TRY(run_kspace(b, b->grid, st));
+    bool grid32_fresh = false;
+    SE_TRY(run_kspace(b, b->grid, st, &grid32_fresh));
     SE_TRY(mark(3));
-    SE_TRY(run_interp(b, b->grid, out, phi, st, b->fft32));
+    SE_TRY(run_interp(b, b->grid, out, phi, st, b->fft32, grid32_fresh));
     SE_TRY(mark(4));
     return SE_OK;
 }
@@ -1496,7 +1565,7 @@ extern "C" int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path)
                              cfg->precision != SE_FP32_FFT32))
         return SE_ERR_INVALID;
     if (path == SE_PATH_TUNE) SE_TRY(tune_path(cfg, &path));
-    if (path < 0 || path > 15) return SE_ERR_INVALID;
+    if (path < 0 || path > 31) return SE_ERR_INVALID;
     se_plan p = new se_plan_s();
     p->cfg = *cfg;
     const int r = batch_create(&p->b, &s, 1, cfg->precision, &path);

@@ -46,7 +46,7 @@ def test_paths_the_configuration_does_not_allow(env):
     with pytest.raises(L.SEError):
         S.SpectralEwald(32, 21, 1.0, 6.0, None, "force", "fp64", 100, path=2)  # P > 16
     with pytest.raises(L.SEError):
-        S.SpectralEwald(32, 8, 1.0, 6.0, None, "force", "fp32", 100, path=16)
+        S.SpectralEwald(32, 8, 1.0, 6.0, None, "force", "fp32", 100, path=32)
     se = S.SpectralEwald(24, 8, 1.0, 6.0, None, "force", "fp32", 100, path=4)
     assert se.path == 4
     assert S.SpectralEwald(32, 8, 1.0, 6.0, None, "force", "fp32", 100).path == 3
