@@ -116,10 +116,13 @@ int se_plan_destroy(se_plan plan);
  * three-kernel bin sort used where it fits (<= 8192 fine bins, <= 2^19
  * particles); both give the same permutation, so the results are identical. */
 #define SE_PATH_RADIX_SORT 8
-/* Run the k-space step through cuFFT (D2Z, the scaling pass, Z2D) rather
- * than the three-pass FP64 FFT used for M = 32, 64 and 128; the results agree
- * to rounding (~1e-15 relative). */
-#define SE_PATH_CUFFT 16
+/* Run the FP64 k-space step of grids with M = 32, 64 or 128 as three
+ * passes of this library's own FFT (the scaling fused into the x pass, the
+ * FP32 grid copy written by the inverse pass) instead of cuFFT's D2Z, the
+ * scaling pass and Z2D; the results agree to rounding (~1e-15 relative).
+ * Off by default: on B200 it ties cuFFT on one M = 128 grid and is slower on
+ * batches of many M = 64 grids. */
+#define SE_PATH_FFT3 16
 int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path);
 /* The path the default choice gives a system of grid M and stencil P. */
 int se_default_path(int M, int P);

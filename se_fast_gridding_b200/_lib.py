@@ -89,7 +89,7 @@ SE_OK, SE_ERR_CUDA, SE_ERR_INVALID, SE_ERR_UNSUPPORTED, SE_ERR_NOMEM, SE_ERR_CUF
 SE_WHERE_HOST, SE_WHERE_DEVICE = 0, 1
 SE_PATH_DEFAULT, SE_PATH_TUNE = -1, -2
 SE_PATH_TILE_SPREAD, SE_PATH_PAIR_INTERP, SE_PATH_RUNTIME_P, SE_PATH_RADIX_SORT = 1, 2, 4, 8
-SE_PATH_CUFFT = 16
+SE_PATH_FFT3 = 16
 SE_POTENTIAL, SE_FORCE = 0, 1
 SE_FP64, SE_FP32, SE_FP32_FFT32 = 0, 1, 2
 

@@ -37,7 +37,7 @@ constexpr int PATH_TILE_SPREAD = 1;    // k_spread2 (else k_spread)
 constexpr int PATH_PAIR_INTERP = 2;    // k_interp2 (else k_interp / k_interp_global)
 constexpr int PATH_RUNTIME_P = 4;      // interpolation without the P-unrolled variants
 constexpr int PATH_RADIX_SORT = 8;     // the batch sorts with the radix passes (se_sort.cu)
-constexpr int PATH_CUFFT = 16;         // the batch's FFTs through cuFFT (not se_fft.cuh)
+constexpr int PATH_FFT3 = 16;          // the batch's FP64 FFTs through se_fft.cuh (not cuFFT)
 
 // The default path: the tile-aligned spread wherever it applies, and the
 // window-pair interpolation from P = 8 on (for shorter stencils its

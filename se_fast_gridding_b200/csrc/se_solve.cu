@@ -840,11 +840,11 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         e = cudaMemcpy(b->fft_tw, tw, sizeof(tw), cudaMemcpyHostToDevice);
     }
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaMemcpy", __FILE__, __LINE__));
-    // the three-pass FFT takes the FP64 transforms of M = 32, 64, 128
-    bool cufft_all = fft32;
+    // on request, the three-pass FFT takes the FP64 transforms of M = 32, 64, 128
+    bool fft3 = false;
     for (int i = 0; i < nsys; i++)
-        if (b->host_sys[i].path & PATH_CUFFT) cufft_all = true;
-    for (auto& g : b->groups) g.custom = !cufft_all && (g.M == 32 || g.M == 64 || g.M == 128);
+        if (b->host_sys[i].path & PATH_FFT3) fft3 = !fft32;
+    for (auto& g : b->groups) g.custom = fft3 && (g.M == 32 || g.M == 64 || g.M == 128);
     for (auto& g : b->groups) {
         if (g.custom) continue;
         int n[3] = {g.M, g.M, g.M};

@@ -1,7 +1,7 @@
-"""The three-pass FP64 k-space step (M = 32, 64, 128) against cuFFT's D2Z,
-scaling and Z2D (SE_PATH_CUFFT): whole solves agree to rounding in both
-modes and precisions, alone and in batches that mix both kinds of group,
-and the step entry point (se_kspace) agrees as well."""
+"""The three-pass FP64 k-space step (SE_PATH_FFT3; M = 32, 64, 128) against
+cuFFT's D2Z, scaling and Z2D: whole solves agree to rounding in both modes
+and precisions, alone and in batches that mix both kinds of group, and the
+step entry point (se_kspace) agrees as well."""
 import numpy as np
 import pytest
 
@@ -31,7 +31,7 @@ def test_three_pass_fft_equals_cufft(env, M, P, mode, prec):
     xd, qd = torch.tensor(x, device="cuda"), torch.tensor(q, device="cuda")
     path = S.default_path(M, P)
     a = S.SpectralEwald(M, P, 1.7, 9.0 / 1.7, None, mode, prec, N)
-    b = S.SpectralEwald(M, P, 1.7, 9.0 / 1.7, None, mode, prec, N, path=path | L.SE_PATH_CUFFT)
+    b = S.SpectralEwald(M, P, 1.7, 9.0 / 1.7, None, mode, prec, N, path=path | L.SE_PATH_FFT3)
     oa, ob = a.solve(xd, qd).cpu().numpy(), b.solve(xd, qd).cpu().numpy()
     assert rel(oa, ob) < (1e-13 if prec == "fp64" else 1e-7), rel(oa, ob)
     # the k-space step alone, on the same grid
@@ -45,9 +45,9 @@ def test_three_pass_fft_equals_cufft(env, M, P, mode, prec):
 
 
 def test_batch_mixing_three_pass_and_cufft_groups(env):
-    """M = 48 and 96 go through cuFFT, 32/64/128 through the three passes,
-    in one batch; every system agrees with its cuFFT-only solve and equals
-    its single-system solve bit for bit."""
+    """With SE_PATH_FFT3, M = 48 and 96 still go through cuFFT and 32/64/128
+    through the three passes, in one batch; every system agrees with the
+    cuFFT-only batch, which equals each single-system solve bit for bit."""
     torch, S, W, L = env
     Ms = [32, 48, 64, 96, 128, 64]
     systems = [S.System(N=900 + 500 * i, M=M, P=(8, 12, 16)[i % 3], L=1.0 + 0.3 * i,
@@ -56,7 +56,7 @@ def test_batch_mixing_three_pass_and_cufft_groups(env):
     xs, qs = zip(*[W.synthetic_system(s.N, s.L, seed=50 + i) for i, s in enumerate(systems)])
     a = S.BatchSolver(systems, "fp64")
     b = S.BatchSolver(systems, "fp64",
-                      paths=[S.default_path(s.M, s.P) | L.SE_PATH_CUFFT for s in systems])
+                      paths=[S.default_path(s.M, s.P) | L.SE_PATH_FFT3 for s in systems])
     x, q = a.pack(xs, qs)
     oa, ob = a.solve(x, q), b.solve(x, q)
     for i, (pa, pb) in enumerate(zip(a.split(oa), b.split(ob))):
