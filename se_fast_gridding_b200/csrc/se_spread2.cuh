@@ -281,10 +281,17 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
             if (n > 0) cp_async_wait<1>();
             else cp_async_wait<0>();
             __syncwarp();
-            const Spread2Stage<Acc>& st = sm.stage[warp][buf ^ 1];
+            Spread2Stage<Acc>& st = sm.stage[warp][buf ^ 1];
+            // lane i scales its particle's 4 y entries by the charge, once
+            if (lane < pending) {
+                const Acc qv = (Acc)st.q[lane];
+#pragma unroll
+                for (int k = 0; k < 4; k++) st.py[lane][k] = st.py[lane][k] * qv;
+            }
+            __syncwarp();
 #pragma unroll 2
             for (int i = 0; i < pending; i++) {
-                const Acc y = st.py[i][ly] * (Acc)st.q[i];
+                const Acc y = st.py[i][ly];
                 acc.add(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
             }
             if constexpr (FOLD) {
