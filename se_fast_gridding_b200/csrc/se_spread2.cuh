@@ -10,16 +10,16 @@
 // most the home tile and the next one (periodically), and the row of tile
 // home + h is R[16h .. 16h + 15]: one aligned 64-byte copy, no wrap logic.
 //
-// One CTA of 4 warps owns one 16^3 tile; warp w owns its y planes 4w..4w+3
-// (all 16 x and z), and after the CTA has listed the bin segments that reach
-// the tile the warps run independently, with no CTA barrier: each warp walks
-// the candidates of the segments in order, keeps the particles whose stencil
-// meets its planes (and the tile in x and z), and streams them in groups --
-// one particle per lane -- through two shared-memory stages that cp.async
-// fills from the factor rows while the warp works on the other: the x and z
-// tile rows, the warp's 4 y entries and the charge.  Each lane adds
-// px[x] * (q py[y] pz[z]) into 16 x 2 cells (all 16 x of its (y, z) and
-// (y, z + 1)).  Every cell belongs to one lane of one CTA: no atomics and a
+// One CTA of 4 warps owns one 16^3 tile; warp w = 2 wy + wz owns the
+// 16 x 8 x 8 block of y in 8 wy + [0, 8) and z in 8 wz + [0, 8), and after
+// the CTA has listed the bin segments that reach the tile the warps run
+// independently, with no CTA barrier: each warp walks the candidates of the
+// segments in order, keeps the particles whose stencil meets its block, and
+// streams them in groups -- one particle per lane -- through two
+// shared-memory stages that cp.async fills from the factor rows while the
+// warp works on the other: the x tile row, the warp's 8 y and 8 z entries and
+// the charge.  Each lane adds px[x] * (q py[y] pz[z]) into 16 x 2 cells (all
+// 16 x of its (y, z) and (y, z + 1)).  Every cell belongs to one lane of one CTA: no atomics and a
 // fixed order of summation (the particles' candidate order).  FP32:
 // packed FP32 pair FMAs on the cells, and after every 512 of the warp's
 // particles the FP32 sums are added into the FP64 grid in place (the first
@@ -38,8 +38,8 @@ constexpr int s2_group() { return sizeof(Acc) == 4 ? 32 : 16; }
 template <typename Acc>
 struct Spread2Stage {
     Acc px[s2_group<Acc>()][16];
-    Acc pz[s2_group<Acc>()][16];
-    Acc py[s2_group<Acc>()][4];
+    Acc pz[s2_group<Acc>()][8];
+    Acc py[s2_group<Acc>()][8];
     double q[s2_group<Acc>()];
 };
 
@@ -177,8 +177,9 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
     const int x0 = tix * 16, y0 = tiy * 16, z0 = tiz * 16;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int ly = lane >> 3, lz = (lane & 7) * 2;
-    const unsigned wbits = 0xFu << (warp * 4);
+    const int wy = warp >> 1, wz = warp & 1;
+    const int ly = lane >> 2, lz = (lane & 3) * 2;
+    const unsigned ybits = 0xFFu << (8 * wy), zbits = 0xFFu << (8 * wz);
 
     // ---- the bin segments reaching this tile (at most 5 x 5 x 2) and their prefix
     const BinRanges rx = bins_reaching(x0, 16, M, P, S.nf[0]);
@@ -222,7 +223,8 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
     int2* list = sm.list[warp];
     double* gs = grid + S.grid_off;
     const long long plane = (long long)M * M;
-    double* cell0 = gs + (long long)x0 * plane + (long long)(y0 + warp * 4 + ly) * M + z0 + lz;
+    double* cell0 =
+        gs + (long long)x0 * plane + (long long)(y0 + 8 * wy + ly) * M + z0 + 8 * wz + lz;
 
     Spread2Accum<Acc> acc;
     acc.zero();
@@ -238,11 +240,13 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
                 while (sl + 1 < nseg && sm.seg_pre[sl + 1] <= pos) sl++;
                 part = sm.seg_beg[sl] + (pos - sm.seg_pre[sl]);
                 pk = sg[part];
-                const int gy = g_of(pk, 1);
-                const int hy = tile_half(gy, tiy, nt, P);
-                const bool meets = tile_half(g_of(pk, 0), tix, nt, P) >= 0 &&
-                                   tile_half(g_of(pk, 2), tiz, nt, P) >= 0 && hy >= 0 &&
-                                   ((((pmask << (gy & 15)) >> (16 * hy)) & 0xFFFFu) & wbits);
+                // the stencil's cells in this tile, as 16-bit masks per axis
+                const int gy = g_of(pk, 1), gz = g_of(pk, 2);
+                const int hy = tile_half(gy, tiy, nt, P), hz = tile_half(gz, tiz, nt, P);
+                const bool meets = tile_half(g_of(pk, 0), tix, nt, P) >= 0 && hy >= 0 &&
+                                   hz >= 0 &&
+                                   ((((pmask << (gy & 15)) >> (16 * hy)) & 0xFFFFu) & ybits) &&
+                                   ((((pmask << (gz & 15)) >> (16 * hz)) & 0xFFFFu) & zbits);
                 if (!meets) part = -1;
             }
             const unsigned keep = __ballot_sync(0xffffffffu, part >= 0);
@@ -264,12 +268,12 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
                 const int hz = tile_half(g_of(e.y, 2), tiz, nt, P);
                 const Acc* r = rows + (long long)e.x * 96;
 #pragma unroll
-                for (int k = 0; k < 16; k += V) {
-                    cp_async16(&st.px[lane][k], r + 16 * hx + k);
-                    cp_async16(&st.pz[lane][k], r + 64 + 16 * hz + k);
-                }
+                for (int k = 0; k < 16; k += V) cp_async16(&st.px[lane][k], r + 16 * hx + k);
 #pragma unroll
-                for (int k = 0; k < 4; k += V) cp_async16(&st.py[lane][k], r + 32 + 16 * hy + 4 * warp + k);
+                for (int k = 0; k < 8; k += V) {
+                    cp_async16(&st.py[lane][k], r + 32 + 16 * hy + 8 * wy + k);
+                    cp_async16(&st.pz[lane][k], r + 64 + 16 * hz + 8 * wz + k);
+                }
                 cp_async8(&st.q[lane], &srec[e.x].w);
             }
             cp_async_commit();
@@ -282,11 +286,11 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
             else cp_async_wait<0>();
             __syncwarp();
             Spread2Stage<Acc>& st = sm.stage[warp][buf ^ 1];
-            // lane i scales its particle's 4 y entries by the charge, once
+            // lane i scales its particle's 8 y entries by the charge, once
             if (lane < pending) {
                 const Acc qv = (Acc)st.q[lane];
 #pragma unroll
-                for (int k = 0; k < 4; k++) st.py[lane][k] = st.py[lane][k] * qv;
+                for (int k = 0; k < 8; k++) st.py[lane][k] = st.py[lane][k] * qv;
             }
             __syncwarp();
 #pragma unroll 2
