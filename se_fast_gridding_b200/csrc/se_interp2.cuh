@@ -14,7 +14,8 @@
 // two neighbouring cells feeds two packed FMAs per accumulator against the
 // particle's z weights, which are zero-padded pairs in registers aligned to
 // the window.  Columns combine with the x (and y) weights in the working
-// precision; the lanes' sums are reduced in FP64 with shuffles.
+// precision; the lanes' sums are reduced in FP64 with shuffles (the four
+// FORCE sums of the FP32 kernel together, warp_sum4).
 //
 // Shared-memory pitches (row Ep, plane PL) come from the host, chosen so that
 // the pair loads of one instruction fall in distinct banks.
@@ -58,6 +59,27 @@ struct Pair<double> {
     __device__ __forceinline__ static double sum(V v) { return v.x + v.y; }
     __device__ __forceinline__ static V zero() { return make_double2(0.0, 0.0); }
 };
+
+// The warp's sums of four values, in lane 0: the first two levels halve the
+// vector (each lane keeps two of the four, then one, and adds its partner's
+// copy of those), the last three add the one kept, and lanes 8, 16, 24 hand
+// lane 0 the sums of the other three.
+__device__ __forceinline__ void warp_sum4(double& v0, double& v1, double& v2, double& v3)
+{
+    const int lane = threadIdx.x & 31;
+    const bool h16 = lane & 16, h8 = lane & 8;
+    const double k0 = h16 ? v2 : v0, k1 = h16 ? v3 : v1;
+    const double w0 = k0 + __shfl_xor_sync(0xffffffffu, h16 ? v0 : v2, 16);
+    const double w1 = k1 + __shfl_xor_sync(0xffffffffu, h16 ? v1 : v3, 16);
+    double u = (h8 ? w1 : w0) + __shfl_xor_sync(0xffffffffu, h8 ? w0 : w1, 8);
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) u += __shfl_xor_sync(0xffffffffu, u, o);
+    // lane l now holds the sum of value 2 (l >> 4 & 1) + (l >> 3 & 1)
+    v0 = u;
+    v1 = __shfl_sync(0xffffffffu, u, 8);
+    v2 = __shfl_sync(0xffffffffu, u, 16);
+    v3 = __shfl_sync(0xffffffffu, u, 24);
+}
 
 // z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
 __host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
@@ -201,11 +223,15 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
             }
             d_pot *= wyj;
         }
-        d_pot = warp_sum(d_pot);
-        if (force) {
-            d_fx = warp_sum(d_fx);
-            d_fy = warp_sum(d_fy);
-            d_fz = warp_sum(d_fz);
+        if (force && sizeof(T) == 4) {   // (the FP64 kernel has no registers to spare)
+            warp_sum4(d_pot, d_fx, d_fy, d_fz);
+        } else {
+            d_pot = warp_sum(d_pot);
+            if (force) {
+                d_fx = warp_sum(d_fx);
+                d_fy = warp_sum(d_fy);
+                d_fz = warp_sum(d_fz);
+            }
         }
         if (lane == 0)
             interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz,
