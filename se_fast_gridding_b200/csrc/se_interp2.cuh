@@ -181,37 +181,47 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
             }
         }
         T a_pot = 0, a_fx = 0, a_fy = 0, a_fz = 0;
-        for (int c = lane; c < P * P; c += 32) {
-            const int i = c / P, j = c - (c / P) * P;
-            const T* col = tile + (r0 + i) * PL + (r1 + j) * Ep + 2 * q0;
-            VT s0 = PV::zero(), s1 = PV::zero();
+        // the columns, summing NQC z pairs each
+        auto columns = [&](auto nqc) {
+            constexpr int NQC = decltype(nqc)::value;
+            for (int c = lane; c < P * P; c += 32) {
+                const int i = c / P, j = c - (c / P) * P;
+                const T* col = tile + (r0 + i) * PL + (r1 + j) * Ep + 2 * q0;
+                VT s0 = PV::zero(), s1 = PV::zero();
 #pragma unroll
-            for (int q = 0; q < NQ; q++) {
-                if (PT || q < nq) {
-                    const VT g2 = PV::load(col + 2 * q);
-                    s0 = PV::fma(g2, wz2[q], s0);
-                    if (force) s1 = PV::fma(g2, fz2[q], s1);
+                for (int q = 0; q < NQC; q++) {
+                    if (PT || q < nq) {
+                        const VT g2 = PV::load(col + 2 * q);
+                        s0 = PV::fma(g2, wz2[q], s0);
+                        if (force) s1 = PV::fma(g2, fz2[q], s1);
+                    }
+                }
+                const T t0 = PV::sum(s0);
+                const T wxi = W.wx[i];
+                if (JFIX) {   // j is the lane's own: the y weights multiply once below
+                    a_pot = fma(t0, wxi, a_pot);
+                    if (force) {
+                        a_fx = fma(t0, W.fx[i], a_fx);
+                        a_fz = fma(PV::sum(s1), wxi, a_fz);
+                    }
+                } else {
+                    const T wyj = W.wy[j];
+                    const T wij = wxi * wyj;
+                    a_pot = fma(t0, wij, a_pot);
+                    if (force) {
+                        a_fx = fma(t0, W.fx[i] * wyj, a_fx);
+                        a_fy = fma(t0, wxi * W.fy[j], a_fy);
+                        a_fz = fma(PV::sum(s1), wij, a_fz);
+                    }
                 }
             }
-            const T t0 = PV::sum(s0);
-            const T wxi = W.wx[i];
-            if (JFIX) {   // j is the lane's own: the y weights multiply once below
-                a_pot = fma(t0, wxi, a_pot);
-                if (force) {
-                    a_fx = fma(t0, W.fx[i], a_fx);
-                    a_fz = fma(PV::sum(s1), wxi, a_fz);
-                }
-            } else {
-                const T wyj = W.wy[j];
-                const T wij = wxi * wyj;
-                a_pot = fma(t0, wij, a_pot);
-                if (force) {
-                    a_fx = fma(t0, W.fx[i] * wyj, a_fx);
-                    a_fy = fma(t0, wxi * W.fy[j], a_fy);
-                    a_fz = fma(PV::sum(s1), wij, a_fz);
-                }
-            }
-        }
+        };
+        // an even stencil that starts on a pair spans P/2 pairs, not P/2 + 1
+        // (a warp-uniform choice: the pair the other form adds is zero)
+        if (PT != 0 && PT % 2 == 0 && (r2 & 1) == 0)
+            columns(std::integral_constant<int, (PT ? PT / 2 : 1)>{});
+        else
+            columns(std::integral_constant<int, NQ>{});
         double d_pot = a_pot, d_fx = a_fx, d_fy = a_fy, d_fz = a_fz;
         if (JFIX) {
             const int j = lane % P;
