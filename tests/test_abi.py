@@ -124,3 +124,15 @@ def test_default_path_without_gpu(L):
     assert L.se_default_path(64, 6) == 1
     assert L.se_default_path(24, 8) == 0
     assert L.se_default_path(128, 21) == 0
+
+
+def test_path_constants_match_the_header():
+    """The SE_PATH_* bits the Python layer passes are the header's."""
+    import re
+    from se_fast_gridding_b200 import _lib
+    hdr = open(os.path.join(ROOT, "include", "se_gpu.h")).read()
+    defs = dict(re.findall(r"#define (SE_PATH_\w+) \(?(-?\d+)\)?", hdr))
+    for name, value in defs.items():
+        assert getattr(_lib, name) == int(value), name
+    assert {"SE_PATH_TILE_SPREAD", "SE_PATH_PAIR_INTERP", "SE_PATH_RUNTIME_P",
+            "SE_PATH_RADIX_SORT", "SE_PATH_FFT3"} <= set(defs)
