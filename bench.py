@@ -8,6 +8,7 @@ Green's-function scaling.  A step is one full solve (sort, spread + fold,
 D2Z, scaling, Z2D, unfold + interpolation) of that system.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1|c2|c3|c4|c5] [--no-extra]
 
 Timing: W untimed steps, then K steps each timed with CUDA events on the
 solve's stream; a 256 MiB buffer is written between steps so every step
@@ -20,6 +21,12 @@ the max over ranks.  `e2e` repeats the measurement through se_solve_host with
 pinned host buffers (H2D of x, q and D2H of the forces inside the timed
 region).  `--impl reference` times SE_fast_gridding's own CPU spectral_ewald()
 (built from its sources) on all host cores instead.
+
+On one GPU the line also carries the other configurations of the metric as
+sub-records, each with its own timing, accuracy and roofline: `c3` (256
+batched POTENTIAL systems), `c4` (the serving loop under Poisson arrivals:
+solves/s, p50/p99) and `c5` (16M clustered FORCE particles, M = 512).
+`--workload cN` prints that configuration alone as its own line.
 """
 from __future__ import annotations
 
@@ -39,11 +46,19 @@ WORKLOAD = dict(N=100_000, M=128, P=16, L=1.0, xi=20.0, mode="force", precision=
                 charges="uniform", seed=1)
 METRIC = "SE3P particles/s at rel-RMS<=1e-6 vs FP64 oracle; serve solves/s, p50/p99"
 FALLBACK_HBM_GBS = 6650.0
+STAGES = ("sort", "spread", "kspace", "interp")
 
 
 def workload_name(w):
     return (f"SE3P {w['mode'].upper()} N={w['N']} M={w['M']}^3 P={w['P']} xi={w['xi']} "
-            f"L={w['L']}, {w['precision'].upper()} gridding (compensated), FP64 FFT+scaling")
+            f"L={w['L']}, rel-RMS<=1e-6 vs the FP64 path")
+
+
+def workload_config(w):
+    """The configuration both arms report (what is solved, not how)."""
+    return {"workload": workload_name(w), "N": w["N"], "M": w["M"], "P": w["P"],
+            "xi": w["xi"], "L": w["L"], "mode": w["mode"],
+            "l2": "GPU arm: flushed between steps (256 MiB write); CPU arm: not applicable"}
 
 
 def dist_env():
@@ -137,37 +152,78 @@ def ncu_traffic():
         return json.load(f)
 
 
-def c3_systems(seed=3):
-    """256 independent POTENTIAL systems: N log-uniform in [1e3, 6.4e4], L in
-    [1, 4], M = 64 (h = L/64), P from {8, 12, 16}, xi = 8/L, charges +-1."""
-    import numpy as np
-    rng = np.random.Generator(np.random.Philox(seed))
-    out = []
-    for i in range(256):
-        N = int(round(np.exp(rng.uniform(np.log(1e3), np.log(6.4e4)))))
-        L = float(rng.uniform(1.0, 4.0))
-        P = int(rng.choice([8, 12, 16]))
-        out.append(dict(N=N, M=64, P=P, L=L, xi=8.0 / L, seed=1000 + i))
-    return out
+_FMA_PEAK = None
 
 
-def run_batched(args):
-    """C3: 256 systems per step, one sort / spread / interpolation launch and
-    one batched cuFFT plan for all of them (FP32 gridding, FP64 k-space)."""
-    import numpy as np
+def fma_peak():
+    global _FMA_PEAK
+    if _FMA_PEAK is None:
+        from se_fast_gridding_b200 import solver
+        _FMA_PEAK = solver.fma_peak_tflops()
+    return _FMA_PEAK
+
+
+def kernel_work(stage, systems, precision):
+    """Algorithmic bytes and flops of one launch of the spread or the
+    interpolation over `systems` ((N, M, P, mode) tuples):
+      spread  bytes N (3 + 1) 8 (positions, charge) + M^3 8 (the FP64 grid,
+              written once, fold fused); flops 2 P^3 N (one FMA per point);
+      interp  bytes M^3 s (the grid, s = 4 on the FP32 path, which reads its
+              FP32 copy) + N 32 + N 8 w (w = 1 POTENTIAL, 3 FORCE);
+              flops 2 P^3 N POTENTIAL, 4 P^3 N FORCE (two FMAs per point:
+              the value and the derivative-weighted sum along z)."""
+    s_grid = 4 if precision.startswith("fp32") else 8
+    b = f = 0.0
+    for N, M, P, mode in systems:
+        w = 3 if mode == "force" else 1
+        if stage == "spread":
+            b += N * 32 + M ** 3 * 8
+            f += 2.0 * P ** 3 * N
+        else:
+            b += M ** 3 * s_grid + N * 32 + N * 8 * w
+            f += (4.0 if mode == "force" else 2.0) * P ** 3 * N
+    return b, f
+
+
+def roofline_of(stage_ms, systems, precision, kname, traffic=None):
+    """Rooflines of the dominant kernel (spread or interpolation, whichever
+    took longer): HBM (algorithmic bytes / stage time) against the measured
+    copy bandwidth, and FP32 FMA (algorithmic flops / stage time) against
+    the measured FMA-chain peak."""
+    hbm, kind = measured_peaks()
+    dom = max(("spread", "interp"), key=lambda k: stage_ms[k])
+    b, f = kernel_work(dom, systems, precision)
+    t = stage_ms[dom] * 1e-3
+    peak_f = fma_peak()
+    return ({"kernel": kname(dom), "bound": "hbm", "achieved": b / t / 1e9, "peak": hbm,
+             "unit": "GB/s", "frac": b / t / 1e9 / hbm,
+             "traffic": None if traffic is None else traffic.get(dom),
+             "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured"
+             else "fallback 6650 GB/s", "algorithmic_bytes": b},
+            {"kernel": kname(dom), "bound": "fp32_fma", "achieved": f / t / 1e12, "peak": peak_f,
+             "unit": "TFLOP/s", "frac": f / t / 1e12 / peak_f, "algorithmic_flops": f,
+             "peak_source": "measured FMA-chain kernel (se_probe_fma_tflops)"})
+
+
+def tile_kernels(M, P):
+    return M % 16 == 0 and M >= 32 and P <= 16
+
+
+def avg_stages(stages):
+    return {k: sum(d[k] for d in stages) / len(stages) for k in STAGES}
+
+
+# ------------------------------------------------------------------- C3 --
+
+def c3_record(args, dev, pg=None, rank=0, world=1):
+    """256 systems per step, one sort / spread / interpolation launch and one
+    batched cuFFT plan for all of them (FP32 gridding, FP64 k-space); the same
+    systems as an FP64 batch and one by one on FP64 single-system plans."""
     import torch
     from se_fast_gridding_b200 import shard, solver
-    from se_fast_gridding_b200 import workloads as O
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
-        pg = dist
-    allsys = c3_systems()
+    from se_fast_gridding_b200 import workloads as W
+    t_start = time.perf_counter()
+    allsys = W.c3_systems()
     mine = shard.partition([solver.System(s["N"], s["M"], s["P"], s["L"], s["xi"]) for s in allsys],
                            world)[rank]
     systems = [solver.System(allsys[i]["N"], 64, allsys[i]["P"], allsys[i]["L"], allsys[i]["xi"])
@@ -175,43 +231,44 @@ def run_batched(args):
     xs, qs = [], []
     for i in mine:
         s = allsys[i]
-        x, q = O.synthetic_system(s["N"], s["L"], seed=s["seed"])
+        x, q = W.synthetic_system(s["N"], s["L"], seed=s["seed"])
         xs.append(x)
         qs.append(q)
-    b = solver.BatchSolver(systems, precision="fp32")
-    x, q = b.pack(xs, qs, device=dev)
-    out = torch.empty(int(b.out_off[-1]), dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    b.set_timing(True)
-    for _ in range(args.warmup):
-        b.solve(x, q, out)
-    torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
-    ms = []
-    stage = {"sort": [], "spread": [], "kspace": [], "interp": []}
-    launches = 0
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        b.solve(x, q, out)
-        e1.record(stream)
-        e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
-        launches += b.launches
-        for kk, v in b.stage_ms().items():
-            stage[kk].append(v)
-    t = sum(ms) / len(ms)
-    if pg:
-        t = shard.max_over_ranks(t)
-    ntot_all = sum(s["N"] for s in allsys)
-    # the plain FP64 single-system path on the same inputs: one plan per
-    # system, the systems solved one after another (L2 flushed first); and the
-    # accuracy of the FP32 batch against it
-    errs = []
-    outs = b.split(out)
+
+    def timed_batch(prec, steps, warmup):
+        b = solver.BatchSolver(systems, precision=prec)
+        x, q = b.pack(xs, qs, device=dev)
+        out = torch.empty(int(b.out_off[-1]), dtype=torch.float64, device=dev)
+        b.set_timing(True)
+        for _ in range(warmup):
+            b.solve(x, q, out)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        ms, st, launches = [], [], 0
+        for k in range(steps):
+            flush.fill_(float(k))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.solve(x, q, out)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            launches += b.launches
+            st.append(b.stage_ms())
+        outs = [o.cpu().numpy() for o in b.split(out)]
+        b.close()
+        t = sum(ms) / len(ms)
+        if pg:
+            t = shard.max_over_ranks(t)
+        return t, avg_stages(st), launches, outs
+
+    t32, st32, launches, o32 = timed_batch("fp32", args.steps, max(args.warmup, 3))
+    t64b, st64b, _, o64 = timed_batch("fp64", 5, 3)
+    # the plain FP64 single-system path: one plan per system, the systems
+    # solved one after another (L2 flushed first)
     plans = [solver.SpectralEwald(s.M, s.P, s.L, s.xi, None, "potential", "fp64", s.N)
              for s in systems]
     xd = [torch.tensor(v, device=dev) for v in xs]
@@ -232,137 +289,188 @@ def run_batched(args):
     fp64_ms = sum(t64) / len(t64)
     if pg:
         fp64_ms = shard.max_over_ranks(fp64_ms)
-    for j in range(len(systems)):
-        errs.append(O.rel_rms(outs[j].cpu().numpy(), od[j].cpu().numpy()))
+    errs = [W.rel_rms(a, b) for a, b in zip(o32, o64)]
     for se in plans:
         se.close()
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": ntot_all / (t * 1e-3), "unit": "particles/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
-            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)",
-            "config": {"workload": "C3 batched SE3P POTENTIAL: 256 systems, N log-uniform "
-                                   "[1e3, 6.4e4], L in [1,4], M=64, P in {8,12,16}, xi=8/L, "
-                                   "FP32 gridding, FP64 k-space, one launch set",
-                       "systems": 256, "particles": ntot_all,
-                       "l2": "flushed between steps (256 MiB write)"},
-            "solves_per_s": 256 / (t * 1e-3), "stage_ms": {k: sum(v) / len(v) for k, v in stage.items()},
-            "gpu_launches": launches,
-            "accuracy": {"rel_rms_fp32_vs_fp64_max_over_systems": max(errs)},
-            "fp64_plain": {"ms_per_step": fp64_ms, "fp32_batched_speedup": fp64_ms / t,
-                           "note": "the same systems solved one by one on FP64 single-system "
-                                   "plans (3 steps, L2 flushed)"},
-        }
-        print(json.dumps(line), flush=True)
-    b.close()
-    if pg:
-        pg.destroy_process_group()
+    ntot_all = sum(s["N"] for s in allsys)
+    info = [(s.N, s.M, s.P, "potential") for s in systems]
+    roof, roof_fma = roofline_of(st32, info, "fp32", lambda d: f"k_{d}2")
+    return {
+        "workload": "256 batched SE3P POTENTIAL systems: N log-uniform [1e3, 6.4e4], L in [1,4], "
+                    "M=64, P in {8,12,16}, xi=8/L, FP32 gridding, FP64 k-space, one launch set",
+        "systems": 256, "particles": ntot_all, "ms_per_step": t32,
+        "particles_per_s": ntot_all / (t32 * 1e-3), "solves_per_s": 256 / (t32 * 1e-3),
+        "stage_ms": st32, "gpu_launches": launches, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "l2": "flushed between steps (256 MiB write)",
+        "accuracy": {"rel_rms_fp32_vs_fp64_max_over_systems": max(errs)},
+        "fp64_batch": {"ms_per_step": t64b, "stage_ms": st64b,
+                       "fp32_speedup": t64b / t32},
+        "fp64_plain": {"ms_per_step": fp64_ms, "fp32_batched_speedup": fp64_ms / t32,
+                       "note": "the same systems solved one by one on FP64 single-system "
+                               "plans (3 steps, L2 flushed)"},
+        "roofline": roof, "roofline_fma": roof_fma,
+        "wall_s": time.perf_counter() - t_start,
+    }
 
 
-def run_large(args):
-    """C5: one clustered FORCE system, N = 16M (64 Gaussian clusters of width
-    0.02 L), M = 512^3, P = 12, xi = 60, FP32 gridding, FP64 k-space."""
-    import numpy as np
+# ------------------------------------------------------------------- C5 --
+
+def c5_record(args, dev, rank=0):
+    """One clustered FORCE system, N = 16M (64 Gaussian clusters of width
+    0.02 L), M = 512^3, P = 12, xi = 60, FP32 gridding, FP64 k-space; its
+    inputs (512 MB) exceed L2, so no flush is needed between steps."""
     import torch
     from se_fast_gridding_b200 import solver
-    from se_fast_gridding_b200 import workloads as O
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    N, M, P, xi = 16_000_000, 512, 12, 60.0
-    x_np, q_np = O.synthetic_system(N, 1.0, seed=5 + rank, charges="pm1", clusters=64, sigma=0.02)
+    from se_fast_gridding_b200 import workloads as W
+    t_start = time.perf_counter()
+    c = W.C5
+    N, M, P, xi = c["N"], c["M"], c["P"], c["xi"]
+    x_np, q_np = W.synthetic_system(N, c["L"], seed=c["seed"] + rank, charges="pm1",
+                                    clusters=c["clusters"], sigma=c["sigma"])
     x, q = torch.tensor(x_np, device=dev), torch.tensor(q_np, device=dev)
-    se = solver.SpectralEwald(M, P, 1.0, xi, None, "force", "fp32", N)
-    out = torch.empty(3 * N, dtype=torch.float64, device=dev)
-    se.set_timing(True)
+    del x_np, q_np
     stream = torch.cuda.current_stream(dev)
-    for _ in range(max(1, args.warmup)):
-        se.solve(x, q, out)
-    ms, stage = [], {"sort": [], "spread": [], "kspace": [], "interp": []}
-    for k in range(args.steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        se.solve(x, q, out)
-        e1.record(stream)
-        e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
-        for kk, v in se.stage_ms().items():
-            stage[kk].append(v)
-    t = sum(ms) / len(ms)
-    # accuracy on a 2,000-particle subset: FP32 vs the FP64 path
-    s64 = solver.SpectralEwald(M, P, 1.0, xi, None, "force", "fp64", N)
-    f64 = s64.solve(x, q)
+
+    def timed(prec, steps, warmup):
+        se = solver.SpectralEwald(M, P, c["L"], xi, None, "force", prec, N)
+        out = torch.empty(3 * N, dtype=torch.float64, device=dev)
+        se.set_timing(True)
+        for _ in range(warmup):
+            se.solve(x, q, out)
+        ms, st = [], []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            se.solve(x, q, out)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            st.append(se.stage_ms())
+        launches = se.launches
+        se.close()
+        return sum(ms) / len(ms), avg_stages(st), out, launches
+
+    steps = max(3, min(args.steps, 10))
+    t32, st32, f32, launches = timed("fp32", steps, 3)
+    t64, st64, f64, _ = timed("fp64", 3, 1)
     idx = torch.arange(0, N, N // 2000, device=dev)[:2000]
-    sub32 = torch.cat([out[idx + d * N] for d in range(3)]).cpu().numpy()
+    sub32 = torch.cat([f32[idx + d * N] for d in range(3)]).cpu().numpy()
     sub64 = torch.cat([f64[idx + d * N] for d in range(3)]).cpu().numpy()
-    err = O.rel_rms(sub32, sub64)
-    if rank == 0:
-        print(json.dumps({
-            "metric": METRIC, "value": world * N / (t * 1e-3), "unit": "particles/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded clustered)",
-            "config": {"workload": "C5 clustered SE3P FORCE N=16e6 (64 clusters, sigma 0.02 L) "
-                                   "M=512^3 P=12 xi=60, FP32 gridding, FP64 k-space",
-                       "N": N, "M": M, "P": P},
-            "stage_ms": {k: sum(v) / len(v) for k, v in stage.items()},
-            "accuracy": {"rel_rms_fp32_vs_fp64_2000": err},
-        }), flush=True)
+    err = W.rel_rms(sub32, sub64)
+    del f32, f64, x, q
+    torch.cuda.empty_cache()
+    roof, roof_fma = roofline_of(st32, [(N, M, P, "force")], "fp32", lambda d: f"k_{d}2")
+    return {
+        "workload": "clustered SE3P FORCE N=16e6 (64 Gaussian clusters, sigma 0.02 L) M=512^3 "
+                    "P=12 xi=60, FP32 gridding, FP64 k-space",
+        "N": N, "M": M, "P": P, "ms_per_step": t32, "particles_per_s": N / (t32 * 1e-3),
+        "stage_ms": st32, "gpu_launches": launches, "steps": steps, "warmup": 3,
+        "l2": "inputs (512 MB) and grid (1 GB) exceed L2",
+        "accuracy": {"rel_rms_fp32_vs_fp64_2000": err},
+        "fp64": {"ms_per_step": t64, "stage_ms": st64, "fp32_speedup": t64 / t32},
+        "roofline": roof, "roofline_fma": roof_fma,
+        "wall_s": time.perf_counter() - t_start,
+    }
 
 
-def run_serve(args):
-    """C4: Poisson arrivals of POTENTIAL/FORCE solves (50/50), N log-uniform in
+# ------------------------------------------------------------------- C4 --
+
+def c4_record(args, dev, rank=0):
+    """Poisson arrivals of POTENTIAL/FORCE solves (50/50), N log-uniform in
     [500, 2e6], P in {8, 12, 16}, through the native request loop (8 slots,
     120 GB budget), host (pinned) inputs and outputs; the results go to one
     pinned buffer made before any replay.  Each trace is replayed once untimed
     (plan cache warm) and once timed; latency is submit to result-in-host-
-    memory on the host clock."""
+    memory on the host clock.  `capacity` submits a whole trace at once (the
+    throughput the loop sustains when requests never wait to arrive), and
+    `fp64_plain` solves the trace's first requests one by one on FP64
+    single-system plans (device buffers, device time) for comparison."""
     import torch
-    from se_fast_gridding_b200 import serve
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
+    from se_fast_gridding_b200 import serve, solver
+    t_start = time.perf_counter()
     xs, qs = serve.particle_pool()
     rates = [2000.0] if args.serve_rates is None else [float(r) for r in args.serve_rates.split(",")]
-    runs = []
     traces = [(literal, rate, serve.poisson_trace(rate, args.serve_seconds, seed=4 + rank,
                                                   literal_grid=literal))
               for literal in (False, True) for rate in rates]
-    # pinned result buffers for the largest trace, made before any replay
     arena = serve.output_arena(max((t for _, _, t in traces),
                                    key=lambda tr: sum(r.system.out_width * r.system.N
                                                       for r in tr)))
+    runs, capacity = [], []
     with serve.Server(slots=args.serve_slots, precision="fp32", hbm_budget=120 * 10 ** 9) as srv:
         for literal, rate, trace in traces:
             serve.replay(srv, trace, xs, qs, arena)                       # warm
             comps, _, wall, lag = serve.replay(srv, trace, xs, qs, arena)  # timed
             parts = sum(r.system.N for r in trace)
             lat = serve.latency_summary(comps)
-            runs.append({"grid": "M=64 for all" if literal else "M=64*2^ceil(log2(N/16000)/3) <= 256",
-                         "offered_req_s": rate, "requests": len(trace),
+            grid = "M=64 for all" if literal else "M=64*2^ceil(log2(N/16000)/3) <= 256"
+            runs.append({"grid": grid, "offered_req_s": rate, "requests": len(trace),
                          "solves_per_s": len(comps) / wall, "particles_per_s": parts / wall,
                          "wall_s": wall, "max_submit_lag_ms": lag * 1e3, **lat})
+            if rate == rates[0]:
+                burst = [serve.TraceRequest(0.0, r.system, r.offset) for r in trace]
+                comps, _, wall, _ = serve.replay(srv, burst, xs, qs, arena)
+                capacity.append({"grid": grid, "requests": len(burst),
+                                 "solves_per_s": len(comps) / wall,
+                                 "particles_per_s": parts / wall, "wall_s": wall})
         st = srv.stats()
-    head = runs[rates.index(2000.0) if 2000.0 in rates else 0]
-    if rank == 0:
-        print(json.dumps({
-            "metric": METRIC, "value": head["solves_per_s"] * world, "unit": "solves/s",
-            "n_gpus": world, "steps": 1, "warmup": 1, "ms_per_step": head["wall_s"] * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded Poisson trace; particles sliced from a uniform pool)",
-            "config": {"workload": f"C4 serving: Poisson {head['offered_req_s']:.0f} req/s for "
-                                   f"{args.serve_seconds} s, POTENTIAL/FORCE 50/50, N log-uniform "
-                                   "[500, 2e6], P in {8,12,16}, L=1, xi=8M/64, FP32 gridding, "
-                                   f"{args.serve_slots} slots, 120 GB budget, pinned host I/O",
-                       "latency_clock": "host steady clock, submit to result in host memory"},
-            "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
-            "particles_per_s": head["particles_per_s"], "runs": runs,
-            "server": {k: st[k] for k in ("plans", "plans_created", "plans_evicted", "hbm_peak")},
-        }), flush=True)
+    # the plain FP64 single-system path on the first requests of the
+    # M-from-N trace: device buffers, one plan per (M, P, mode), device time
+    trace = traces[0][2][:128]
+    stream = torch.cuda.current_stream(dev)
+    plans = {}
+    xd = xs.to(dev)
+    qd = qs.to(dev)
+    outs = {}
+    for r in trace:
+        s = r.system
+        key = (s.M, s.P, s.mode)
+        cap = max(rr.system.N for rr in trace if (rr.system.M, rr.system.P, rr.system.mode) == key)
+        if key not in plans:
+            plans[key] = solver.SpectralEwald(s.M, s.P, s.L, s.xi, None, s.mode, "fp64", cap)
+        outs.setdefault(key, torch.empty(3 * cap, dtype=torch.float64, device=dev))
+
+    def run_plain():
+        for r in trace:
+            s = r.system
+            key = (s.M, s.P, s.mode)
+            plans[key].solve_system(s, xd[r.offset:r.offset + 3 * s.N], qd[r.offset:r.offset + s.N],
+                                    outs[key][:s.out_width * s.N])
+    run_plain()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run_plain()
+    e1.record(stream)
+    e1.synchronize()
+    t64 = e0.elapsed_time(e1) * 1e-3
+    parts64 = sum(r.system.N for r in trace)
+    for p in plans.values():
+        p.close()
+    del xd, qd, outs
+    head = runs[0]
+    cap0 = capacity[0]
+    return {
+        "workload": f"serving: Poisson {head['offered_req_s']:.0f} req/s for {args.serve_seconds} s, "
+                    "POTENTIAL/FORCE 50/50, N log-uniform [500, 2e6], P in {8,12,16}, L=1, "
+                    f"xi=8M/64, FP32 gridding, {args.serve_slots} slots, 120 GB budget, "
+                    "pinned host I/O",
+        "latency_clock": "host steady clock, submit to result in host memory",
+        "solves_per_s": head["solves_per_s"], "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
+        "particles_per_s": head["particles_per_s"], "runs": runs, "capacity": capacity,
+        "fp64_plain": {"requests": len(trace), "particles_per_s": parts64 / t64,
+                       "solves_per_s": len(trace) / t64,
+                       "served_capacity_speedup": cap0["particles_per_s"] / (parts64 / t64),
+                       "note": "the first 128 requests of the M-from-N trace solved one by one "
+                               "on FP64 single-system plans, device buffers, device time"},
+        "server": {k: st[k] for k in ("plans", "plans_created", "plans_evicted", "hbm_peak")},
+        "wall_s": time.perf_counter() - t_start,
+    }
 
 
-def run_c1(args):
-    """C1: plain SE3P POTENTIAL FP64, N=100 charges +-1 in the unit box, M=32,
+# ------------------------------------------------------------------- C1 --
+
+def c1_record(args, dev):
+    """Plain SE3P POTENTIAL FP64, N=100 charges +-1 in the unit box, M=32,
     P=21, xi=8, m=0.94 sqrt(pi P) -- the reference's CPU-runnable case.  A
     solve this small is bound by launches: timed directly, replayed from a
     CUDA graph (se_plan_set_graph), through host buffers, and the reference's
@@ -370,9 +478,6 @@ def run_c1(args):
     import torch
     from se_fast_gridding_b200 import solver
     from se_fast_gridding_b200 import workloads as W
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     N, M, P, xi = 100, 32, 21, 8.0
     x_np, q_np = W.synthetic_system(N, 1.0, seed=0, charges="pm1")
     m = 0.94 * (3.14159265358979323846 * P) ** 0.5
@@ -415,19 +520,23 @@ def run_c1(args):
                    "kind": r["kind"], "sample": r["sample"]}
         except Exception as e:   # reported, not required
             cpu = {"sample": f"failed: {e}"[:200]}
-    if rank == 0:
-        best = res["graph"]
-        print(json.dumps({
-            "metric": METRIC, "value": N / (best * 1e-3), "unit": "particles/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": best,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded, charges +-1)",
-            "config": {"workload": "C1 SE3P POTENTIAL FP64 N=100 M=32^3 P=21 xi=8 L=1",
-                       "timing": "CUDA events over back-to-back solves on one stream"},
-            "us_per_solve": {k: 1e3 * v for k, v in res.items()},
-            "cpu_reference": cpu,
-        }), flush=True)
+    return {"us_per_solve": {k: 1e3 * v for k, v in res.items()}, "cpu_reference": cpu,
+            "ms_per_step": res["graph"], "steps": args.steps, "warmup": max(args.warmup, 3),
+            "workload": "SE3P POTENTIAL FP64 N=100 M=32^3 P=21 xi=8 L=1",
+            "particles_per_s": N / (res["graph"] * 1e-3)}
 
+
+def sub_line(rec, value_key, unit, n_gpus, dtype):
+    """A standalone JSON line for one configuration's record."""
+    return {"metric": METRIC, "value": rec[value_key] * n_gpus, "unit": unit, "n_gpus": n_gpus,
+            "steps": rec.get("steps", 1), "warmup": rec.get("warmup", 1),
+            "ms_per_step": rec["ms_per_step"] if "ms_per_step" in rec else rec["wall_s"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded)", "config": {"workload": rec["workload"]},
+            **{k: v for k, v in rec.items() if k != "workload"}}
+
+
+# ------------------------------------------------------------ reference --
 
 def run_reference_arm(args):
     rank, world, _ = dist_env()
@@ -439,49 +548,65 @@ def run_reference_arm(args):
     res = cpu_reference(args, procs, 1, args.steps, args.warmup, w)
     value = res["value"]
     ms = 1e3 * sum(res["step_s"]) / len(res["step_s"])
+    fft = res.get("fft")
+    excl = None
+    if fft:
+        excl = {"value": procs * w["N"] / (fft["solve_s"] - fft["fft_s_per_solve"]),
+                "unit": "particles/s", "fft_share": fft["share"],
+                "fft_s_per_solve": fft["fft_s_per_solve"], "solve_s": fft["solve_s"],
+                "note": "the same solves with the time inside fftw_execute (the project's own "
+                        "mixed-radix CPU FFT standing in for the absent FFTW) taken out"}
     line = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded uniform charges and positions)",
-        "config": {"workload": workload_name(dict(w, precision="fp64")) + " (CPU reference)",
-                   "N": w["N"], "M": w["M"], "P": w["P"], "xi": w["xi"]},
+        "config": workload_config(w),
         "impl": "reference",
+        "arithmetic": "FP64 gridding and FFT (the reference's AVX path, -DFGG_SPLIT -DFORCE)",
         "cpu_baseline": {"value": value, "unit": "particles/s", "cores": res["cores"],
                          "kind": res["kind"], "sample": res["sample"]},
+        "excluding_fft": excl,
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-procs", type=int, default=0,
-                    help="CPU processes for --impl reference (default: all cores)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
-                    help="c2: the headline single FORCE system; c3: 256 batched systems; "
-                         "c4: the serving loop under Poisson arrivals; c5: 16M clustered particles")
-    ap.add_argument("--serve-seconds", type=float, default=1.0)
-    ap.add_argument("--serve-rates", default=None, help="comma-separated req/s (default 2000)")
-    ap.add_argument("--serve-slots", type=int, default=8)
-    args = ap.parse_args()
-    if args.impl == "reference":
-        return run_reference_arm(args)
-    if args.workload == "c1":
-        return run_c1(args)
-    if args.workload == "c3":
-        return run_batched(args)
-    if args.workload == "c4":
-        return run_serve(args)
-    if args.workload == "c5":
-        return run_large(args)
+# ------------------------------------------------------------------- C2 --
 
+def timed_solves(se, x, q, out, stream, flush, steps):
+    import torch
+    ms, st = [], []
+    for k in range(steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        se.solve(x, q, out)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        st.append(se.stage_ms())
+    return sum(ms) / len(ms), avg_stages(st)
+
+
+def timed_host(se, N, xh, qh, oh, stream, flush, steps, warmup):
+    import torch
+    for _ in range(max(warmup, 1)):
+        se.solve_host_ptr(N, xh.data_ptr(), qh.data_ptr(), oh.data_ptr())
+    ms = []
+    for k in range(steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        se.solve_host_ptr(N, xh.data_ptr(), qh.data_ptr(), oh.data_ptr())
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    return sum(ms) / len(ms)
+
+
+def run_c2(args):
     import numpy as np
     import torch
     from se_fast_gridding_b200 import solver
@@ -511,57 +636,45 @@ def main():
     x = torch.tensor(x_np, device=dev)
     q = torch.tensor(q_np, device=dev)
     out = torch.empty(3 * N, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    xh = torch.tensor(x_np).pin_memory()
+    qh = torch.tensor(q_np).pin_memory()
+    oh = torch.empty(3 * N, dtype=torch.float64).pin_memory()
 
     # accuracy (rank 0, outside the timed region): FP32 vs the FP64 path and
-    # vs the FP64 direct k-space sum on the 1,000-particle subset
-    accuracy = None
-    fp64_ms = None
-    fft32 = None
+    # vs the FP64 direct k-space sum on the 1,000-particle subset; the plain
+    # FP64 path and the FP32-FFT mode timed the same way
+    accuracy = fp64 = fft32 = None
     if rank == 0:
         se.solve(x, q, out)
         f32 = out.cpu().numpy()
         s64 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp64", N)
         s64.set_graph(True)
+        s64.set_timing(True)
         f64 = s64.solve(x, q).cpu().numpy()
-        # the plain FP64 path on the same inputs, timed the same way (the
-        # FP32 path is measured against it)
-        fl = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
         o64 = torch.empty(3 * N, dtype=torch.float64, device=dev)
         for _ in range(3):
             s64.solve(x, q, o64)
-        t64 = []
-        for k in range(5):
-            fl.fill_(float(k))
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            s64.solve(x, q, o64)
-            b.record(stream)
-            b.synchronize()
-            t64.append(a.elapsed_time(b))
-        fp64_ms = sum(t64) / len(t64)
-        # the FP32-FFT mode on the same inputs, timed the same way
+        t64, st64 = timed_solves(s64, x, q, o64, stream, flush, 5)
+        s64.set_timing(False)
+        e2e64 = timed_host(s64, N, xh, qh, oh, stream, flush, 5, 3)
+        fp64 = {"ms_per_step": t64, "stage_ms": st64,
+                "e2e": {"value": N / (e2e64 * 1e-3), "unit": "particles/s", "ms_per_step": e2e64,
+                        "h2d_bytes_per_step": 4 * N * 8, "d2h_bytes_per_step": 3 * N * 8},
+                "note": "the FP64 path on the same inputs, same timing (5 steps, L2 flushed); "
+                        "e2e through se_solve_host with pinned host buffers"}
         s3 = solver.SpectralEwald(w["M"], w["P"], w["L"], w["xi"], m, w["mode"], "fp32-fft32", N)
         s3.set_graph(True)
         o3 = torch.empty(3 * N, dtype=torch.float64, device=dev)
         s3.set_timing(True)
         for _ in range(3):
             s3.solve(x, q, o3)
-        t3, st3 = [], []
-        for k in range(10):
-            fl.fill_(float(k))
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            s3.solve(x, q, o3)
-            b.record(stream)
-            b.synchronize()
-            t3.append(a.elapsed_time(b))
-            st3.append(s3.stage_ms())
+        t3, st3 = timed_solves(s3, x, q, o3, stream, flush, 10)
         f3 = o3.cpu().numpy()
-        fft32 = {"ms_per_step": sum(t3) / len(t3), "value": N / (sum(t3) / len(t3) * 1e-3),
-                 "stage_ms": {k: sum(d[k] for d in st3) / len(st3) for k in st3[0]},
+        fft32 = {"ms_per_step": t3, "value": N / (t3 * 1e-3), "stage_ms": st3,
                  "rel_rms_vs_fp64": O.rel_rms(f3, f64)}
         s3.close()
-        del fl, o64, o3
+        del o64, o3
         s64.close()
         accuracy = {"rel_rms_fp32_vs_fp64": O.rel_rms(f32, f64)}
         gpath = os.path.join(ROOT, "tests", "golden", "c2.npz")
@@ -575,9 +688,8 @@ def main():
             sub3 = np.concatenate([f3[t + d * N] for d in range(3)])
             fft32["rel_rms_vs_direct_1000"] = O.rel_rms(sub3, g["force_direct"])
 
-    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
     se.set_timing(True)
-    for _ in range(args.warmup):
+    for _ in range(max(args.warmup, 3)):
         flush.fill_(1.0)
         se.solve(x, q, out)
     torch.cuda.synchronize()
@@ -588,7 +700,7 @@ def main():
     time.sleep(0.3)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    stage = {"sort": [], "spread": [], "kspace": [], "interp": []}
+    stage = []
     launches = 0
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
@@ -598,8 +710,7 @@ def main():
         se.solve(x, q, out)
         ev[k][1].record(stream)
         launches += se.launches
-        for key, v in se.stage_ms().items():
-            stage[key].append(v)
+        stage.append(se.stage_ms())
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -611,7 +722,7 @@ def main():
         ms = float(t.item())
         pg.barrier()
     value = world * N / (ms * 1e-3)
-    stage_avg = {k: sum(v) / len(v) for k, v in stage.items()}
+    stage_avg = avg_stages(stage)
 
     # the same solves launched directly (no graph), for comparison
     se.set_graph(False)
@@ -629,77 +740,43 @@ def main():
     direct_ms = sum(direct) / len(direct)
 
     # end to end through the host-buffer entry point, pinned buffers
-    xh = torch.tensor(x_np).pin_memory()
-    qh = torch.tensor(q_np).pin_memory()
-    oh = torch.empty(3 * N, dtype=torch.float64).pin_memory()
-    se.set_timing(False)
-    for _ in range(max(args.warmup, 1)):
-        se.solve_host_ptr(N, xh.data_ptr(), qh.data_ptr(), oh.data_ptr())
-    e2e_ms = []
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        se.solve_host_ptr(N, xh.data_ptr(), qh.data_ptr(), oh.data_ptr())
-        b.record(stream)
-        b.synchronize()
-        e2e_ms.append(a.elapsed_time(b))
-    e2e = sum(e2e_ms) / len(e2e_ms)
+    e2e = timed_host(se, N, xh, qh, oh, stream, flush, args.steps, args.warmup)
     if pg:
         t = torch.tensor([e2e], device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e = float(t.item())
+    se.close()
 
     if rank != 0:
         if pg:
             pg.destroy_process_group()
         return
 
-    # roofline of the dominant kernel
-    hbm, hbm_kind = measured_peaks()
-    fma = solver.fma_peak_tflops()
-    s = 4 if w["precision"] == "fp32" else 8
-    P, M = w["P"], w["M"]
-    dom = max(("spread", "interp"), key=lambda k: stage_avg[k])
-    if dom == "spread":
-        alg_bytes = N * 4 * 8 + M ** 3 * 8      # x, q in; M^3 FP64 grid out
-        flops = 2.0 * P ** 3 * N
-    else:
-        alg_bytes = M ** 3 * 8 + N * 4 * 8 + 3 * N * 8
-        flops = 8.0 * P ** 3 * N
-    t_dom = stage_avg[dom] * 1e-3
     tr = ncu_traffic()
-    traffic = None
-    if tr and tr.get("workload") == workload_name(w):
-        traffic = tr.get(dom)
-    kname = f"k_{dom}2" if (M % 16 == 0 and M >= 32 and P <= 16) else f"k_{dom}"
-    roofline = {"kernel": kname, "bound": "hbm", "achieved": alg_bytes / t_dom / 1e9,
-                "peak": hbm, "unit": "GB/s", "frac": alg_bytes / t_dom / 1e9 / hbm,
-                "traffic": traffic, "peak_source": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                if hbm_kind == "measured" else "fallback 6650 GB/s",
-                "algorithmic_bytes": alg_bytes}
-    roofline_fma = {"kernel": kname, "bound": "fp32_fma", "achieved": flops / t_dom / 1e12,
-                    "peak": fma, "unit": "TFLOP/s", "frac": flops / t_dom / 1e12 / fma,
-                    "peak_source": "measured FMA-chain kernel (se_probe_fma_tflops)"}
+    traffic = tr if (tr and tr.get("workload") == workload_name(w)) else None
+    P, M = w["P"], w["M"]
+    tiles = tile_kernels(M, P)
+    roofline, roofline_fma = roofline_of(stage_avg, [(N, M, P, w["mode"])], w["precision"],
+                                         lambda d: f"k_{d}2" if tiles else f"k_{d}", traffic)
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
             res = cpu_reference(args, 1, 1, 1, 0, w)
             cpu = {"value": res["value"], "unit": "particles/s", "cores": res["cores"],
-                   "kind": res["kind"], "sample": res["sample"]}
+                   "kind": res["kind"], "sample": res["sample"], "fft": res.get("fft")}
         except Exception as e:   # the baseline is reported, not required
             cpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference",
                    "sample": f"failed: {e}"[:200]}
     line = {
         "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform charges and positions, one replica per GPU)",
-        "config": {"workload": workload_name(w), "N": N, "M": M, "P": P, "xi": w["xi"],
-                   "L": w["L"], "precision": w["precision"], "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (256 MiB write)",
-                   "launch": "CUDA graph replay on a side stream (se_plan_set_graph); "
-                             "e2e: se_solve_host"},
+        "config": workload_config(w),
+        "arithmetic": "FP32 spread/interpolation with compensated (FP64-folded) sums, FP64 FFT "
+                      "and Green's-function scaling",
+        "parallelism": f"replicas x{world}",
+        "launch": "CUDA graph replay on a side stream (se_plan_set_graph); e2e: se_solve_host",
         "roofline": roofline, "roofline_fma": roofline_fma,
         "stage_ms": stage_avg, "direct_launch_ms_per_step": direct_ms, "cpu_baseline": cpu,
         "e2e": {"value": world * N / (e2e * 1e-3), "unit": "particles/s",
@@ -708,12 +785,63 @@ def main():
         "gpu_launches": launches,
         "clocks": clk, "accuracy": accuracy, "wall_s_timed": wall,
         "fp32_fft32": fft32,
-        "fp64_plain": None if fp64_ms is None else {
-            "ms_per_step": fp64_ms, "fp32_speedup": fp64_ms / ms,
-            "note": "the FP64 path on the same inputs, same timing (5 steps, L2 flushed)"},
+        "fp64_plain": None if fp64 is None else dict(fp64, fp32_speedup=fp64["ms_per_step"] / ms),
     }
+    if world == 1 and not args.no_extra:
+        torch.cuda.empty_cache()
+        line["c3"] = c3_record(args, dev)
+        line["c4"] = c4_record(args, dev)
+        line["c5"] = c5_record(args, dev)
     print(json.dumps(line), flush=True)
-    se.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-procs", type=int, default=0,
+                    help="CPU processes for --impl reference (default: all cores)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="C2 line only, without the c3 / c4 / c5 sub-records")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2: the headline single FORCE system (with c3/c4/c5 sub-records); "
+                         "c3: 256 batched systems; c4: the serving loop under Poisson "
+                         "arrivals; c5: 16M clustered particles; c1: the 100-particle FP64 case")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-rates", default=None, help="comma-separated req/s (default 2000)")
+    ap.add_argument("--serve-slots", type=int, default=8)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    if args.workload == "c2":
+        return run_c2(args)
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if args.workload == "c3" and world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    if args.workload == "c1":
+        rec, key, unit, dtype = c1_record(args, dev), "particles_per_s", "particles/s", "f64"
+    elif args.workload == "c3":
+        rec, key, unit, dtype = c3_record(args, dev, pg, rank, world), "particles_per_s", \
+            "particles/s", "f32"
+    elif args.workload == "c4":
+        rec, key, unit, dtype = c4_record(args, dev, rank), "solves_per_s", "solves/s", "f32"
+    else:
+        rec, key, unit, dtype = c5_record(args, dev, rank), "particles_per_s", "particles/s", "f32"
+    if rank == 0:
+        n = 1 if args.workload == "c3" else world   # c3: the systems are shared out
+        print(json.dumps(sub_line(rec, key, unit, n, dtype)), flush=True)
     if pg:
         pg.destroy_process_group()
 

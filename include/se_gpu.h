@@ -215,7 +215,9 @@ int se_counting_sort(const int* keys, int N, int nkeys, int* perm, int* offsets,
  * library, until exit), so N <= SE_SORT_STATIC_MAX_N and
  * nkeys <= SE_SORT_STATIC_MAX_KEYS; larger sizes return SE_ERR_INVALID.
  * The first call on a device resolves the array's address and should come
- * before any stream capture.  Calls share the array: calls that overlap on
+ * before any stream capture; the address is kept for the life of the
+ * process, which assumes the device's primary context is never reset
+ * (no cudaDeviceReset between calls).  Calls share the array: calls that overlap on
  * the GPU race and must be serialised by the caller.  Results are identical
  * to se_counting_sort. */
 #define SE_SORT_STATIC_MAX_N 262144

@@ -13,7 +13,22 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include "fftw3.h"
+
+/* Wall time spent inside fftw_execute since the last fc_fft_reset(): the CPU
+ * baseline reports the FFT's share of a reference solve with it. */
+static double fc_fft_time;
+
+double fc_fft_seconds(void) { return fc_fft_time; }
+void fc_fft_reset(void) { fc_fft_time = 0; }
+
+static double fc_now(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
 
 #define FC_PI 3.14159265358979323846
 
@@ -181,7 +196,16 @@ fftw_plan fftw_plan_dft_c2r_3d(int n0, int n1, int n2, fftw_complex* in,
     return fc_new(n0, n1, n2, FC_C2R, FFTW_BACKWARD, in, out);
 }
 
+static void fc_execute(const fftw_plan p);
+
 void fftw_execute(const fftw_plan p)
+{
+    const double t0 = fc_now();
+    fc_execute(p);
+    fc_fft_time += fc_now() - t0;
+}
+
+static void fc_execute(const fftw_plan p)
 {
     const long tot = (long)p->n[0] * p->n[1] * p->n[2];
     const int nh = p->n[2] / 2 + 1;

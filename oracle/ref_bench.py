@@ -26,6 +26,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def _worker(rank, args, barrier, q_out):
+    try:
+        _work(rank, args, barrier, q_out)
+    except BaseException as e:   # the parent must not wait for a worker that died
+        barrier.abort()
+        q_out.put((rank, "error", repr(e)))
+
+
+def _work(rank, args, barrier, q_out):
     os.environ["OMP_NUM_THREADS"] = str(args.threads)
     sys.path.insert(0, HERE)
     import numpy as np
@@ -40,8 +48,13 @@ def _worker(rank, args, barrier, q_out):
     devnull = os.open(os.devnull, os.O_WRONLY)
     saved = os.dup(1)
     times = []
+    if kind == "reference":
+        import ctypes as C
+        lib.fc_fft_seconds.restype = C.c_double
     for step in range(args.warmup + args.steps):
         barrier.wait()
+        if kind == "reference":
+            lib.fc_fft_reset()
         t0 = time.perf_counter()
         os.dup2(devnull, 1)          # the reference prints dispatcher lines
         try:
@@ -52,9 +65,10 @@ def _worker(rank, args, barrier, q_out):
         finally:
             os.dup2(saved, 1)
         t1 = time.perf_counter()
+        fft = lib.fc_fft_seconds() if kind == "reference" else None
         barrier.wait()
         if step >= args.warmup:
-            times.append((t0, t1))
+            times.append((t0, t1, fft))
     q_out.put((rank, kind, times))
 
 
@@ -82,6 +96,9 @@ def main(argv=None):
     results = [q_out.get() for _ in procs]
     for p in procs:
         p.join()
+    errors = [r for r in results if r[1] == "error"]
+    if errors:
+        sys.exit(f"reference worker failed: {errors[0][2]}")
     kind = results[0][1]
     step_s = []
     for s in range(args.steps):
@@ -90,10 +107,19 @@ def main(argv=None):
         step_s.append(max(ends) - min(starts))
     per_step = sum(step_s) / len(step_s)
     value = args.procs * args.N / per_step
+    # the FFT's share of one solve (time inside fftw_execute, the project's
+    # own CPU FFT standing in for FFTW), averaged over workers and steps
+    solve_s = [t1 - t0 for r in results for (t0, t1, _) in r[2]]
+    fft_s = [f for r in results for (_, _, f) in r[2] if f is not None]
+    fft = None
+    if fft_s:
+        fft = {"fft_s_per_solve": sum(fft_s) / len(fft_s),
+               "solve_s": sum(solve_s) / len(solve_s),
+               "share": sum(fft_s) / sum(solve_s)}
     print(json.dumps({
         "value": value, "unit": "particles/s", "kind": kind,
         "cores": args.procs * args.threads, "procs": args.procs, "threads": args.threads,
-        "step_s": step_s,
+        "step_s": step_s, "fft": fft,
         "sample": (f"{args.procs} x spectral_ewald() ({args.mode}, N={args.N}, M={args.M}, "
                    f"P={args.P}, xi={args.xi}) per step, {args.steps} steps"),
     }))

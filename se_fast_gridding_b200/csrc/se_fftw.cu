@@ -106,7 +106,10 @@ void fftw_execute(const fftw_plan p)
     if (hin) din = p->din;
     if (hout) dout = inplace ? din : p->dout;
     if (inplace && (hin != hout)) dout = din;   // mixed kinds cannot alias
-    if (e == cudaSuccess && hin) e = cudaMemcpy(din, p->in, p->in_bytes, cudaMemcpyHostToDevice);
+    // an in-place real transform uses FFTW's (and cuFFT's) padded layout:
+    // n0 x n1 x 2(n2/2 + 1) reals, the size of the half spectrum, both ways
+    const size_t in_copy = inplace ? big : p->in_bytes, out_copy = inplace ? big : p->out_bytes;
+    if (e == cudaSuccess && hin) e = cudaMemcpy(din, p->in, in_copy, cudaMemcpyHostToDevice);
     cufftResult r = CUFFT_SUCCESS;
     if (e == cudaSuccess) {
         cufftSetStream(p->h, 0);
@@ -119,7 +122,7 @@ void fftw_execute(const fftw_plan p)
             r = cufftExecZ2D(p->h, (cufftDoubleComplex*)din, (cufftDoubleReal*)dout);
     }
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e == cudaSuccess && hout) e = cudaMemcpy(p->out, dout, p->out_bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && hout) e = cudaMemcpy(p->out, dout, out_copy, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess || r != CUFFT_SUCCESS)
         fprintf(stderr, "[se_gpu] fftw_execute failed: %s / cuFFT %d\n", cudaGetErrorString(e),
                 (int)r);

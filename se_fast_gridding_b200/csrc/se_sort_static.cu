@@ -11,7 +11,10 @@
 //
 // Set-up: the first call on each device looks up the device address of
 // g_sort_scratch with cudaGetSymbolAddress (with that device current) and
-// caches it; make that first call outside any stream capture.  All calls
+// caches it for the life of the process; make that first call outside any
+// stream capture.  The cache assumes the device's primary context lives as
+// long as the process: after a cudaDeviceReset the cached address would
+// belong to a context that no longer exists.  All calls
 // share the array, which keeps the previous call's contents: the sort clears
 // the parts that must start at zero (the bin counts) itself, and calls whose
 // work overlaps on the GPU (different streams, concurrent graphs) race on the

@@ -202,10 +202,14 @@ def fgg_steps(ref: Ref, ref2p: Ref, x, q, M, P, L, xi, m, tag, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SE_REF_DIR"),
+                    help="SE_fast_gridding checkout (default: $SE_REF_DIR)")
     ap.add_argument("--skip-c2", action="store_true")
     ap.add_argument("--realspace-only", action="store_true")
     args = ap.parse_args()
+    if not args.ref or not os.path.isfile(os.path.join(args.ref, "SE_fgg.c")):
+        ap.error("the reference sources are needed: pass --ref <SE_fast_gridding checkout> "
+                 "or set SE_REF_DIR")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={args.ref}", "all", "ref"],
                    check=True)
     if args.realspace_only:

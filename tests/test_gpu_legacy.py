@@ -233,6 +233,22 @@ def test_fftw_shim(F, shape):
     L.fftw_execute(C.c_void_p(pl))
     L.fftw_destroy_plan(C.c_void_p(pl))
     np.testing.assert_allclose(out.reshape(shape), r * r.size, rtol=0, atol=1e-11 * r.size)
+    # in place on a host array: FFTW's padded layout, n0 x n1 x 2(n2/2 + 1)
+    # reals in, the half spectrum out (and back)
+    pad = 2 * (n2 // 2 + 1)
+    ip = np.zeros((n0, n1, pad))
+    ip[:, :, :n2] = r
+    ip = ip.reshape(-1)
+    pl = L.fftw_plan_dft_r2c_3d(n0, n1, n2, F.dptr(ip), F.dptr(ip), 1 << 6)
+    L.fftw_execute(C.c_void_p(pl))
+    L.fftw_destroy_plan(C.c_void_p(pl))
+    got = ip.view(np.complex128).reshape(ref.shape)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    pl = L.fftw_plan_dft_c2r_3d(n0, n1, n2, F.dptr(ip), F.dptr(ip), 1 << 6)
+    L.fftw_execute(C.c_void_p(pl))
+    L.fftw_destroy_plan(C.c_void_p(pl))
+    np.testing.assert_allclose(ip.reshape(n0, n1, pad)[:, :, :n2], r * r.size, rtol=0,
+                               atol=1e-11 * r.size)
 
 
 def test_out_of_box_position_reported(F):

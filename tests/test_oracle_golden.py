@@ -111,6 +111,27 @@ def test_direct_sums_match_reference(oracle_mod):
     phi, f = O.sf_kspace(x, q, 3.1814, 8.0, np.arange(10), jmax=layers, kcut2=-1.0)
     np.testing.assert_allclose(phi, g["N10/direct_phi"], rtol=1e-11)
     np.testing.assert_allclose(f, g["N10/direct_force"], rtol=1e-10, atol=1e-13)
+    # and its torch restatement (the checker of the GPU tests at millions of
+    # particles), here on the CPU
+    phi_t, f_t = O.sf_kspace_torch(x, q, 3.1814, 8.0, np.arange(10), jmax=layers, kcut2=-1.0)
+    np.testing.assert_allclose(phi_t, g["N10/direct_phi"], rtol=1e-11)
+    np.testing.assert_allclose(f_t, g["N10/direct_force"], rtol=1e-10, atol=1e-13)
+
+
+@pytest.mark.parametrize("clusters", [0, 4])
+def test_torch_structure_factor_sum_equals_oracle(oracle_mod, clusters):
+    """sf_kspace_torch = sf_kspace (the C oracle's structure-factor sum) with
+    and without the sphere cut, over several particle chunks."""
+    O = oracle_mod
+    x, q = O.synthetic_system(300, 1.3, seed=3 + clusters, charges="uniform",
+                              clusters=clusters, sigma=0.05)
+    t = np.arange(0, 300, 7)
+    jmax, kc2 = O.kspace_converged_jmax(1.3, 6.0)
+    for cut in (kc2, -1.0):
+        p0, f0 = O.sf_kspace(x, q, 1.3, 6.0, t, jmax, cut)
+        p1, f1 = O.sf_kspace_torch(x, q, 1.3, 6.0, t, jmax, cut, chunk=128)
+        assert O.rel_rms(p1, p0) < 1e-13
+        assert O.rel_rms(f1, f0) < 1e-13
 
 
 def test_reference_accuracy_figures(oracle_mod):

@@ -57,16 +57,38 @@ def test_static_sort_matches_allocating_sort_twice(env):
 
 
 def test_static_sort_limits(env):
-    torch, L, _ = env
+    torch, L, solver = env
     max_n = 262144
     keys = torch.zeros(max_n + 1, dtype=torch.int32, device="cuda")
     rc, _, _ = static_sort(env, keys, 16)
     assert rc != 0
     rc, _, _ = static_sort(env, keys[:16], 65536 + 1)
     assert rc != 0
-    # at the limits it works
+    # at the limits it gives exactly the allocating sort's permutation and
+    # offsets: the size where a short scratch array would show
     keys = torch.tensor(np.random.Generator(np.random.Philox(5)).integers(
         0, 65536, size=max_n).astype(np.int32), device="cuda")
     rc, perm, offs = static_sort(env, keys, 65536)
     assert rc == 0
-    assert torch.equal(perm.sort().values, torch.arange(max_n, dtype=torch.int32, device="cuda"))
+    ref_perm, ref_offs = solver.counting_sort(keys, 65536)
+    torch.cuda.synchronize()
+    assert torch.equal(perm, ref_perm)
+    assert torch.equal(offs, ref_offs)
+
+
+@pytest.mark.parametrize("nkeys", [1, 2])
+def test_static_sort_few_keys_at_max_n(env, nkeys):
+    """All keys equal (the identity permutation) and two keys, at the largest
+    N the array takes."""
+    torch, L, solver = env
+    max_n = 262144
+    keys = torch.tensor(np.random.Generator(np.random.Philox(9 + nkeys)).integers(
+        0, nkeys, size=max_n).astype(np.int32), device="cuda")
+    rc, perm, offs = static_sort(env, keys, nkeys)
+    assert rc == 0
+    ref_perm, ref_offs = solver.counting_sort(keys, nkeys)
+    torch.cuda.synchronize()
+    assert torch.equal(perm, ref_perm)
+    assert torch.equal(offs, ref_offs)
+    if nkeys == 1:
+        assert torch.equal(perm, torch.arange(max_n, dtype=torch.int32, device="cuda"))
