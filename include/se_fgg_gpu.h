@@ -101,6 +101,8 @@ void SE_FGG_pack_params(SE_FGG_params*, int N, int M0, int M1, int M2,
                         int P, double c, double h);            /* SE_fgg.c:69-88   */
 void SE2P_FGG_pack_params(SE_FGG_params*, int N, int M0, int M1, int M2,
                           int P, double c, double h, double a); /* SE_fgg.c:91-110  */
+void SE1P_FGG_pack_params(SE_FGG_params*, int N, int M0, int M1, int M2, int P,
+                          double c, double h, double a, double b); /* SE_fgg.c:113-132 */
 void parse_params(SE_opt*, double xi);                        /* SE_general.c:16-29  */
 void SE_FGG_FCN_params(SE_FGG_params*, const SE_opt*, int N); /* SE_general.c:180-200 */
 double SE_init_params(int* M, int* P, double* m, double eps, double L,
@@ -132,20 +134,24 @@ void SE_FGG_reorder_system(SE_state*, const SE_FGG_work*,
 /* ---- base Gaussian and expansion vectors ------------------------------- */
 void SE_FGG_base_gaussian(SE_FGG_work*, const SE_FGG_params*);            /* SE_fgg.c:508-535 */
 /* Expansion vectors with q = 1 (SE_fgg.c:920-938).  The reference picks the
- * expansion at compile time (-DTHREE_PERIODIC / -DTWO_PERIODIC, SE_fgg.h:17-27);
- * this library uses the 3P expansion (SE_fgg.c:539-621) unless the process was
- * started with SE_GPU_PERIODICITY=2, which selects the 2P one (SE_fgg.c:727-819)
- * for SE_FGG_expand_all, SE_FGG_grid and SE_FGG_int, as -DTWO_PERIODIC does. */
+ * expansion at compile time (-DTHREE_PERIODIC / -DTWO_PERIODIC /
+ * -DONE_PERIODIC, SE_fgg.h:17-33); this library uses the 3P expansion
+ * (SE_fgg.c:539-621) unless the process was started with SE_GPU_PERIODICITY=2
+ * or 1, which selects the 2P one (SE_fgg.c:727-819) or the 1P one
+ * (SE_fgg.c:823-916) for SE_FGG_expand_all, SE_FGG_grid and SE_FGG_int, as
+ * those builds do. */
 void SE_FGG_expand_all(SE_FGG_work*, const SE_state*, const SE_FGG_params*);
 /* FORCE factors, 3P only (the reference defines no 2P force expansion,
  * SE_fgg.h:24-27). */
 void SE_FGG_expand_all_SSE_force(SE_FGG_work*, const SE_state*,
                                  const SE_FGG_params*);                   /* SE_fgg.c:941-963 */
 
-/* 3P / 2P expansion regardless of SE_GPU_PERIODICITY (no counterpart name in
- * the reference; each equals SE_FGG_expand_all of the matching build). */
+/* 3P / 2P / 1P expansion regardless of SE_GPU_PERIODICITY (no counterpart
+ * name in the reference; each equals SE_FGG_expand_all of the matching
+ * build). */
 void SE3P_FGG_expand_all(SE_FGG_work*, const SE_state*, const SE_FGG_params*);
 void SE2P_FGG_expand_all(SE_FGG_work*, const SE_state*, const SE_FGG_params*);
+void SE1P_FGG_expand_all(SE_FGG_work*, const SE_state*, const SE_FGG_params*);
 
 /* ---- spread, POTENTIAL: H[idx+(i,j,k)] += q zx zy zz zs ----------------- */
 void SE_FGG_grid(SE_FGG_work*, const SE_state*, const SE_FGG_params*);      /* SE_fgg.c:3866-3914 */
@@ -177,6 +183,12 @@ void SE_FGG_wrap_fcn(double* H_per, const SE_FGG_work*, const SE_FGG_params*);  
 void SE2P_FGG_wrap_fcn(double* H_per, const SE_FGG_work*, const SE_FGG_params*); /* SE_fgg.c:357-382 */
 void SE_FGG_extend_fcn(SE_FGG_work*, const double* H_per, const SE_FGG_params*); /* SE_fgg.c:417-443 */
 void SE2P_FGG_extend_fcn(SE_FGG_work*, const double* H_per, const SE_FGG_params*); /* SE_fgg.c:448-473 */
+/* 1P (z periodic, x and y free): as the reference, H_per is indexed
+ * i + j M0 + k M0 M1 with the padded i < M0 + P, j < M1 + P, so it must hold
+ * (M0 + P - 1) + (M1 + P - 1) M0 + (M2 - 1) M0 M1 + 1 elements (the map
+ * overlaps itself; overlapping cells sum in the reference's order). */
+void SE1P_FGG_wrap_fcn(double* H_per, const SE_FGG_work*, const SE_FGG_params*); /* SE_fgg.c:387-411 */
+void SE1P_FGG_extend_fcn(SE_FGG_work*, const double* H_per, const SE_FGG_params*); /* SE_fgg.c:478-502 */
 
 /* ---- interpolate, POTENTIAL: phi[m] = h^3 sum H zs zx zy zz ------------- */
 void SE_FGG_int(double* phi, const SE_FGG_work*, const SE_state*, const SE_FGG_params*); /* SE_fgg.c:968-1019 */

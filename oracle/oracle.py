@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
         _lib = C.CDLL(path)
         _lib.orc_expand.restype = C.c_int
         _lib.orc_calc_energy.restype = C.c_double
+        _lib.orc_per_size.restype = C.c_long
     return _lib
 
 
@@ -134,10 +135,13 @@ class Setup:
         return self.opt().eta
 
 
-def pack_params(N, M0, M1, M2, P, c, h, a=-1.0) -> FGGParams:
+def pack_params(N, M0, M1, M2, P, c, h, a=-1.0, b=-1.0) -> FGGParams:
+    """SE_FGG_pack_params / SE2P_FGG_pack_params (offset a of the free z) /
+    SE1P_FGG_pack_params (offsets a, b of the free x, y), SE_fgg.c:69-132."""
     p = FGGParams()
     lib().orc_pack_params(C.byref(p), N, M0, M1, M2, P, C.c_double(c), C.c_double(h),
                           C.c_double(a))
+    p.b = b
     return p
 
 
@@ -192,9 +196,13 @@ def grid(p, x, q, zs, periodicity=3, H=None):
     return H
 
 
+def per_size(p, periodicity=3) -> int:
+    """Elements of the periodic grid of the wrap / extend calls (orc_per_size)."""
+    return int(lib().orc_per_size(C.byref(p), periodicity))
+
+
 def wrap(p, H, periodicity=3, H_per=None):
-    n = p.dims[0] * p.dims[1] * (p.dims[2] if periodicity == 3 else p.npdims[2])
-    H_per = np.zeros(n) if H_per is None else H_per
+    H_per = np.zeros(per_size(p, periodicity)) if H_per is None else H_per
     lib().orc_wrap(dptr(H_per), dptr(H), C.byref(p), periodicity)
     return H_per
 

@@ -111,7 +111,8 @@ void orc_base_gaussian(double* zs, const SE_FGG_params* p)
 
 /* ------------------------------------------------------------- expansion -- */
 
-/* SE_fgg.c:539-621 (3P), :625-722 (3P force), :727-819 (2P). */
+/* SE_fgg.c:539-621 (3P), :625-722 (3P force), :727-819 (2P: z free, offset
+ * a), :823-916 (1P: x and y free, offsets a and b, z periodic). */
 int orc_expand(const double xn[3], double q, const SE_FGG_params* p, int periodicity,
                double* zx, double* zy, double* zz,
                double* zfx, double* zfy, double* zfz)
@@ -122,8 +123,9 @@ int orc_expand(const double xn[3], double q, const SE_FGG_params* p, int periodi
     double t0[3];
     int first[3];
     for (int d = 0; d < 3; d++) {
-        const int shifted = (periodicity == 2 && d == 2);
-        const double s = shifted ? p->a + h / 2 : 0.;
+        const int shifted = (periodicity == 2 && d == 2) || (periodicity == 1 && d < 2);
+        const double off = (periodicity == 1 && d == 1) ? p->b : p->a;
+        const double s = shifted ? off + h / 2 : 0.;
         const double u = shifted ? (xn[d] - s) / h : xn[d] / h;
         const int cell = odd ? (int)round(u) : (int)floor(u);
         first[d] = odd ? cell - ph : cell - (ph - 1);
@@ -145,6 +147,8 @@ int orc_expand(const double xn[3], double q, const SE_FGG_params* p, int periodi
             for (int i = 0; i < P; i++) zf[d][i] = -c * (t0[d] - (lo + i) * h);
     }
     for (int i = 0; i < P; i++) zx[i] *= z3;
+    if (periodicity == 1)   /* :912-915: the free x and y corners are not shifted */
+        return (int)orc_rmaj(first[0], first[1], first[2] + ph, p->npdims[1], p->npdims[2]);
     const int kz = (periodicity == 2) ? first[2] : first[2] + ph;
     return (int)orc_rmaj(first[0] + ph, first[1] + ph, kz, p->npdims[1], p->npdims[2]);
 }
@@ -213,7 +217,22 @@ void orc_grid(double* H, const double* x, const double* q, const double* zs,
 
 /* ----------------------------------------------------------- fold/unfold -- */
 
-/* SE_fgg.c:327-352 (3P) and :357-382 (2P: z is copied, not folded).  The
+/* Elements of the periodic grid the wrap writes and the extend reads: 3P
+ * M0 M1 M2, 2P M0 M1 (M2 + P); 1P the largest index its column-major map
+ * i + j M0 + k M0 M1 reaches for the unfolded i < M0 + P, j < M1 + P (the
+ * reference's SE1P_FGG_wrap_fcn / extend_fcn, SE_fgg.c:387-411, :478-502,
+ * index H_per with the periodic strides M0, M1 over the padded x and y
+ * extents, so the map overlaps itself and runs P M0 + P - 1 past M0 M1 M2). */
+long orc_per_size(const SE_FGG_params* p, int periodicity)
+{
+    const long m0 = p->dims[0], m1 = p->dims[1], m2 = p->dims[2];
+    if (periodicity == 2) return m0 * m1 * p->npdims[2];
+    if (periodicity == 1) return (p->npdims[0] - 1) + (p->npdims[1] - 1) * m0 + (m2 - 1) * m0 * m1 + 1;
+    return m0 * m1 * m2;
+}
+
+/* SE_fgg.c:327-352 (3P), :357-382 (2P: z is copied, not folded) and
+ * :387-411 (1P: only z is folded; x and y keep their padded index).  The
  * += order is the row-major walk of H, as in the reference. */
 void orc_wrap(double* H_per, const double* H, const SE_FGG_params* p, int periodicity)
 {
@@ -221,6 +240,13 @@ void orc_wrap(double* H_per, const double* H, const SE_FGG_params* p, int period
     const int m0 = p->dims[0], m1 = p->dims[1], m2 = p->dims[2];
     const int n0 = p->npdims[0], n1 = p->npdims[1], n2 = p->npdims[2];
     long s = 0;
+    if (periodicity == 1) {
+        for (int i = 0; i < n0; i++)
+            for (int j = 0; j < n1; j++)
+                for (int k = 0; k < n2; k++, s++)
+                    H_per[orc_cmaj(i, j, orc_pmod(k - ph, m2), m0, m1)] += H[s];
+        return;
+    }
     for (int i = 0; i < n0; i++) {
         const int wi = orc_pmod(i - ph, m0);
         for (int j = 0; j < n1; j++) {
@@ -233,13 +259,20 @@ void orc_wrap(double* H_per, const double* H, const SE_FGG_params* p, int period
     }
 }
 
-/* SE_fgg.c:417-443 (3P) and :448-473 (2P) */
+/* SE_fgg.c:417-443 (3P), :448-473 (2P) and :478-502 (1P) */
 void orc_extend(double* H, const double* H_per, const SE_FGG_params* p, int periodicity)
 {
-    const int ph = (periodicity == 2) ? orc_half(p->P) : p->P_half;
+    const int ph = (periodicity == 3) ? p->P_half : orc_half(p->P);
     const int m0 = p->dims[0], m1 = p->dims[1], m2 = p->dims[2];
     const int n0 = p->npdims[0], n1 = p->npdims[1], n2 = p->npdims[2];
     long s = 0;
+    if (periodicity == 1) {
+        for (int i = 0; i < n0; i++)
+            for (int j = 0; j < n1; j++)
+                for (int k = 0; k < n2; k++, s++)
+                    H[s] = H_per[orc_cmaj(i, j, orc_pmod(k - ph, m2), m0, m1)];
+        return;
+    }
     for (int i = 0; i < n0; i++) {
         const int wi = orc_pmod(i - ph, m0);
         for (int j = 0; j < n1; j++) {

@@ -31,7 +31,7 @@ int  orc_init_params(int* M, int* P, double* m, double L, double xi,
 /* base Gaussian zs[P^3] */
 void orc_base_gaussian(double* zs, const SE_FGG_params* p);
 
-/* expansion of one particle; periodicity 3 or 2; zf* may be NULL */
+/* expansion of one particle; periodicity 3, 2 or 1; zf* may be NULL */
 int orc_expand(const double xn[3], double q, const SE_FGG_params* p, int periodicity,
                double* zx, double* zy, double* zz,
                double* zfx, double* zfy, double* zfz);
@@ -47,6 +47,7 @@ void orc_grid(double* H, const double* x, const double* q, const double* zs,
               const SE_FGG_params* p, int periodicity);
 
 /* fold / unfold; H_per column-major */
+long orc_per_size(const SE_FGG_params* p, int periodicity);
 void orc_wrap(double* H_per, const double* H, const SE_FGG_params* p, int periodicity);
 void orc_extend(double* H, const double* H_per, const SE_FGG_params* p, int periodicity);
 

@@ -42,11 +42,16 @@ static void set_error(int code, const char* msg)
     if (code) fprintf(stderr, "[se_gpu] %s\n", msg);
 }
 
+// The periodicity of the names the reference builds per periodicity
+// (SE_FGG_expand_all, SE_FGG_grid, SE_FGG_int: -DTHREE_PERIODIC,
+// -DTWO_PERIODIC or -DONE_PERIODIC, SE_fgg.h:17-33): SE_GPU_PERIODICITY = 2 or
+// 1 selects 2P or 1P, anything else 3P.
 static int periodicity_default()
 {
     static int p = [] {
         const char* e = getenv("SE_GPU_PERIODICITY");
-        return (e && atoi(e) == 2) ? 2 : 3;
+        const int v = e ? atoi(e) : 3;
+        return (v == 2 || v == 1) ? v : 3;
     }();
     return p;
 }
@@ -175,6 +180,21 @@ static size_t nper(const SE_FGG_params* p)
     return (size_t)p->dims[0] * p->dims[1] * p->dims[2];
 }
 
+// Elements of the periodic grid a wrap writes / an extend reads: 3P
+// M0 M1 M2; 2P M0 M1 (M2 + P); 1P the largest index of the reference's
+// column-major map i + j M0 + k M0 M1 over the unfolded i < M0 + P,
+// j < M1 + P (SE_fgg.c:387-411, :478-502 index H_per with the periodic
+// strides M0, M1 over the padded x and y extents, so the map overlaps itself
+// and runs P M0 + P - 1 past M0 M1 M2).
+static long long nper_of(const SE_FGG_params* p, int periodicity)
+{
+    const long long m0 = p->dims[0], m1 = p->dims[1], m2 = p->dims[2];
+    if (periodicity == 2) return m0 * m1 * p->npdims[2];
+    if (periodicity == 1)
+        return (p->npdims[0] - 1) + (p->npdims[1] - 1) * m0 + (m2 - 1) * m0 * m1 + 1;
+    return m0 * m1 * m2;
+}
+
 // ------------------------------------------------------------- kernels ---
 
 __device__ __forceinline__ int vmod_d(int i, int n)
@@ -186,7 +206,7 @@ __device__ __forceinline__ int vmod_d(int i, int n)
 struct ParamsDev {
     int N, P, P_half, lo;   // lo: first stencil offset (-p_half or 1 - p_half)
     int dims[3], npdims[3];
-    double c, d, h, a;
+    double c, d, h, a, b;   // a, b: offsets of the free directions (2P: z; 1P: x, y)
 };
 
 // Set by a kernel that skipped a particle whose stencil leaves the padded
@@ -241,6 +261,7 @@ static ParamsDev to_dev(const SE_FGG_params* p)
     q.d = p->d;
     q.h = p->h;
     q.a = p->a;
+    q.b = p->b;
     return q;
 }
 
@@ -258,7 +279,8 @@ __global__ void k_base_gaussian(double* zs, ParamsDev p)
 }
 
 // One particle's expansion, SE_fgg.c:539-621 (3P), :625-722 (force),
-// :727-819 (2P); q folded into zx.  Returns the padded corner index.
+// :727-819 (2P: z free, offset a), :823-916 (1P: x and y free, offsets a
+// and b); q folded into zx.  Returns the padded corner index.
 __device__ int expand_one(const double xn[3], double q, const ParamsDev& p, int periodicity,
                           double* zx, double* zy, double* zz, double* zfx, double* zfy,
                           double* zfz)
@@ -268,8 +290,8 @@ __device__ int expand_one(const double xn[3], double q, const ParamsDev& p, int 
     double t0[3];
     int first[3];
     for (int d = 0; d < 3; d++) {
-        const bool sh = periodicity == 2 && d == 2;
-        const double s = sh ? p.a + p.h / 2 : 0.0;
+        const bool sh = (periodicity == 2 && d == 2) || (periodicity == 1 && d < 2);
+        const double s = sh ? (periodicity == 1 && d == 1 ? p.b : p.a) + p.h / 2 : 0.0;
         const double u = sh ? (xn[d] - s) / p.h : xn[d] / p.h;
         const int cell = odd ? (int)round(u) : (int)floor(u);
         first[d] = odd ? cell - ph : cell - (ph - 1);
@@ -290,6 +312,8 @@ __device__ int expand_one(const double xn[3], double q, const ParamsDev& p, int 
             for (int i = 0; i < P; i++) zf[d][i] = -p.c * (t0[d] - (p.lo + i) * p.h);
     }
     for (int i = 0; i < P; i++) zx[i] *= z3;
+    if (periodicity == 1)   // the free x and y corners are not shifted (:912-915)
+        return (first[0] * p.npdims[1] + first[1]) * p.npdims[2] + first[2] + ph;
     const int kz = periodicity == 2 ? first[2] : first[2] + ph;
     return ((first[0] + ph) * p.npdims[1] + first[1] + ph) * p.npdims[2] + kz;
 }
@@ -365,8 +389,8 @@ __global__ void k_grid_vanilla(double* H, const double* __restrict__ x,
     }
 }
 
-// SE_fgg.c:327-352 / :357-382 as a gather: each periodic cell adds its padded
-// pre-images in the reference's row-major order.
+// SE_fgg.c:327-352 / :357-382 / :387-411 as a gather: each periodic cell adds
+// its padded pre-images in the reference's row-major order.
 __global__ void k_wrap(double* H_per, const double* __restrict__ H, ParamsDev p,
                        int periodicity, long long nout)
 {
@@ -375,6 +399,22 @@ __global__ void k_wrap(double* H_per, const double* __restrict__ H, ParamsDev p,
     const int m0 = p.dims[0], m1 = p.dims[1], m2 = p.dims[2];
     const int n0 = p.npdims[0], n1 = p.npdims[1], n2 = p.npdims[2];
     const int ph = (p.P & 1) ? (p.P - 1) / 2 : p.P / 2;
+    if (periodicity == 1) {
+        // pre-images (i, j, k) of c = i + m0 (j + m1 w), w = vmod(k - ph, m2),
+        // i < n0, j < n1, k < n2, walked with i, then j, then k ascending
+        double acc = H_per[c];
+        for (long long i = c % m0; i < n0 && i <= c; i += m0) {
+            const long long sv = (c - i) / m0;   // j + m1 w
+            for (long long j = sv % m1; j < n1 && j <= sv; j += m1) {
+                const long long w = (sv - j) / m1;
+                if (w >= m2) continue;
+                const long long row = (i * n1 + j) * n2;
+                for (int k = vmod_d((int)w + ph, m2); k < n2; k += m2) acc += H[row + k];
+            }
+        }
+        H_per[c] = acc;
+        return;
+    }
     const int wi = (int)(c % m0);
     const int wj = (int)((c / m0) % m1);
     const int wk = (int)(c / ((long long)m0 * m1));
@@ -391,7 +431,7 @@ __global__ void k_wrap(double* H_per, const double* __restrict__ H, ParamsDev p,
     H_per[c] = acc;
 }
 
-// SE_fgg.c:417-443 / :448-473
+// SE_fgg.c:417-443 / :448-473 / :478-502
 __global__ void k_extend(double* H, const double* __restrict__ H_per, ParamsDev p,
                          int periodicity, int ph)
 {
@@ -400,6 +440,10 @@ __global__ void k_extend(double* H, const double* __restrict__ H_per, ParamsDev 
     if (t >= (long long)n0 * n1 * n2) return;
     const int k = (int)(t % n2), j = (int)((t / n2) % n1), i = (int)(t / ((long long)n1 * n2));
     const int m0 = p.dims[0], m1 = p.dims[1], m2 = p.dims[2];
+    if (periodicity == 1) {
+        H[t] = H_per[i + (long long)m0 * (j + (long long)m1 * vmod_d(k - ph, m2))];
+        return;
+    }
     const int wi = vmod_d(i - ph, m0), wj = vmod_d(j - ph, m1);
     const int wk = periodicity == 2 ? k : vmod_d(k - ph, m2);
     H[t] = H_per[wi + (long long)m0 * (wj + (long long)m1 * wk)];
@@ -701,8 +745,7 @@ static int do_grid_vanilla(SE_FGG_work* w, const SE_state* st, const SE_FGG_para
 static int do_wrap(double* H_per, const SE_FGG_work* w, const SE_FGG_params* p, int periodicity)
 {
     if (!H_per || !w || !w->H || !valid_params(p)) return SE_ERR_INVALID;
-    const long long nout = (long long)p->dims[0] * p->dims[1] *
-                           (periodicity == 2 ? p->npdims[2] : p->dims[2]);
+    const long long nout = nper_of(p, periodicity);
     Stager s;
     double* Hp = (double*)s.use(H_per, (size_t)nout * 8, true, true);
     const double* H = (const double*)s.use(w->H, npad(p) * 8, true, false);
@@ -715,13 +758,12 @@ static int do_extend(SE_FGG_work* w, const double* H_per, const SE_FGG_params* p
                      int periodicity)
 {
     if (!H_per || !w || !w->H || !valid_params(p)) return SE_ERR_INVALID;
-    const long long nin = (long long)p->dims[0] * p->dims[1] *
-                          (periodicity == 2 ? p->npdims[2] : p->dims[2]);
+    const long long nin = nper_of(p, periodicity);
     Stager s;
     double* H = (double*)s.use(w->H, npad(p) * 8, false, true);
     const double* Hp = (const double*)s.use(H_per, (size_t)nin * 8, true, false);
     SE_TRY(s.copy_in());
-    const int ph = periodicity == 2 ? ((p->P & 1) ? (p->P - 1) / 2 : p->P / 2) : p->P_half;
+    const int ph = periodicity == 3 ? p->P_half : ((p->P & 1) ? (p->P - 1) / 2 : p->P / 2);
     k_extend<<<blocks((long long)npad(p), 256), 256>>>(H, Hp, to_dev(p), periodicity, ph);
     return s.finish();
 }
@@ -893,6 +935,14 @@ void SE2P_FGG_pack_params(SE_FGG_params* params, int N, int M0, int M1, int M2, 
 {
     SE_FGG_pack_params(params, N, M0, M1, M2, P, c, h);
     params->a = a;
+}
+
+void SE1P_FGG_pack_params(SE_FGG_params* params, int N, int M0, int M1, int M2, int P,
+                          double c, double h, double a, double b)
+{
+    SE_FGG_pack_params(params, N, M0, M1, M2, P, c, h);
+    params->a = a;
+    params->b = b;
 }
 
 void parse_params(SE_opt* opt, double xi)
@@ -1151,6 +1201,11 @@ void SE2P_FGG_expand_all(SE_FGG_work* w, const SE_state* st, const SE_FGG_params
     report(do_expand(w, st, p, 2, false), "SE2P_FGG_expand_all");
 }
 
+void SE1P_FGG_expand_all(SE_FGG_work* w, const SE_state* st, const SE_FGG_params* p)
+{
+    report(do_expand(w, st, p, 1, false), "SE1P_FGG_expand_all");
+}
+
 void SE_FGG_expand_all_SSE_force(SE_FGG_work* w, const SE_state* st, const SE_FGG_params* p)
 {
     report(do_expand(w, st, p, 3, true), "SE_FGG_expand_all_SSE_force");
@@ -1201,6 +1256,11 @@ void SE2P_FGG_wrap_fcn(double* H_per, const SE_FGG_work* w, const SE_FGG_params*
     report(do_wrap(H_per, w, p, 2), "SE2P_FGG_wrap_fcn");
 }
 
+void SE1P_FGG_wrap_fcn(double* H_per, const SE_FGG_work* w, const SE_FGG_params* p)
+{
+    report(do_wrap(H_per, w, p, 1), "SE1P_FGG_wrap_fcn");
+}
+
 void SE_FGG_extend_fcn(SE_FGG_work* w, const double* H_per, const SE_FGG_params* p)
 {
     report(do_extend(w, H_per, p, 3), "SE_FGG_extend_fcn");
@@ -1209,6 +1269,11 @@ void SE_FGG_extend_fcn(SE_FGG_work* w, const double* H_per, const SE_FGG_params*
 void SE2P_FGG_extend_fcn(SE_FGG_work* w, const double* H_per, const SE_FGG_params* p)
 {
     report(do_extend(w, H_per, p, 2), "SE2P_FGG_extend_fcn");
+}
+
+void SE1P_FGG_extend_fcn(SE_FGG_work* w, const double* H_per, const SE_FGG_params* p)
+{
+    report(do_extend(w, H_per, p, 1), "SE1P_FGG_extend_fcn");
 }
 
 // ---- interpolate, POTENTIAL ----

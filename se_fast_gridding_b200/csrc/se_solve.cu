@@ -379,6 +379,14 @@ struct se_batch_s {
     void* fac = nullptr;      // per-particle factors [ntot][3][PS], working precision
     int PS = 0;
     void* rows = nullptr;     // tile-aligned rows [ntot][3][32] (k_spread2 systems)
+    // k_spread2's split of crowded tiles: parts per tile (scanned), the
+    // per-tile completion counters, the block counter of k_tile_parts, the
+    // FP64 slabs of the parts after the first, and the launch bound
+    int* tile_parts = nullptr;
+    int* tile_done = nullptr;
+    unsigned* tp_counter = nullptr;
+    double* slab = nullptr;
+    int slab_slots = 0;
     bool any_spread1 = false, any_spread2 = false;   // some system on k_spread / k_spread2
     bool any_interp1 = false, any_interp2 = false;   // on k_interp(_global) / k_interp2
     bool runtime_p = false;                          // some system asks for runtime P
@@ -504,6 +512,14 @@ static int path_of(const se_system* sys, const int* paths, int i)
     return paths ? paths[i] : default_path(sys[i].M, sys[i].P);
 }
 
+// Slab slots k_spread2 may need for the particles of its systems: a bin is a
+// candidate of at most 2 tiles per axis, so the candidates of all tiles sum
+// to at most 8 N and the parts after each tile's first to 8 N / S2_CAP.
+static int split_slots(long long ntile2)
+{
+    return (int)(8 * ntile2 / S2_CAP) + 1;
+}
+
 static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nbins_out,
                           int* ntiles_out, const int* paths = nullptr)
 {
@@ -534,6 +550,11 @@ static size_t batch_bytes(const se_system* sys, int nsys, int precision, int* nb
     }
     if (plain) b += (size_t)ntot * 3 * maxP * (precision == SE_FP32 ? 4 : 8);
     if (rows) b += (size_t)ntot * 3 * 32 * (precision == SE_FP32 ? 4 : 8);
+    long long ntile2 = 0;
+    for (int i = 0; i < nsys; i++)
+        if (path_of(sys, paths, i) & PATH_TILE_SPREAD) ntile2 += sys[i].N;
+    if (ntile2 > 0 || rows)
+        b += (size_t)split_slots(ntile2) * 4096 * 8 + (size_t)(2 * ntiles + 2) * 4;
     if ((pair && precision == SE_FP32) || fft32) b += (size_t)grid * 4;   // FP32 grids
     b += std::max(sort_scratch_bytes((int)ntot, (int)std::max<long long>(nbins, 1)),
                   bsort_scratch_bytes((int)std::max<long long>(nbins, 1)));
@@ -570,7 +591,8 @@ static int batch_free(se_batch b)
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
                     b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows,
-                    b->grid32, b->spec32, b->d_order, b->fft_tw};
+                    b->grid32, b->spec32, b->d_order, b->fft_tw, b->tile_parts,
+                    b->tile_done, b->tp_counter, b->slab};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -789,6 +811,16 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     }
     if (need_fac) SE_ALLOC(b->fac, nt * 3 * b->PS * (precision == SE_FP32 ? 4 : 8));
     if (need_rows) SE_ALLOC(b->rows, nt * 3 * 32 * (precision == SE_FP32 ? 4 : 8));
+    if (b->any_spread2) {
+        long long ntile2 = 0;
+        for (int i = 0; i < nsys; i++)
+            if (b->host_sys[i].path & PATH_TILE_SPREAD) ntile2 += systems[i].N;
+        b->slab_slots = split_slots(ntile2);
+        SE_ALLOC(b->tile_parts, sizeof(int) * (b->ntiles + 1));
+        SE_ALLOC(b->tile_done, sizeof(int) * std::max(b->ntiles, 1));
+        SE_ALLOC(b->tp_counter, sizeof(unsigned));
+        SE_ALLOC(b->slab, sizeof(double) * 4096 * (size_t)b->slab_slots);
+    }
     if ((b->any_interp2 && precision == SE_FP32) || fft32)
         SE_ALLOC(b->grid32, sizeof(float) * (b->grid_elems + 16));
     if (fft32) SE_ALLOC(b->spec32, sizeof(float2) * b->spec_elems);
@@ -827,6 +859,9 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         e = cudaMemcpy(b->d_bin_prefix, b->bin_prefix.data(), sizeof(int) * (nsys + 1),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(b->err, 0, sizeof(int));
+    if (e == cudaSuccess && b->tile_done)
+        e = cudaMemset(b->tile_done, 0, sizeof(int) * std::max(b->ntiles, 1));
+    if (e == cudaSuccess && b->tp_counter) e = cudaMemset(b->tp_counter, 0, sizeof(unsigned));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_order, order.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
@@ -939,14 +974,24 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
 {
     // every tile is written by exactly one of the two kernels (by system)
     if (b->any_spread2) {
+        // the parts of each tile, then one CTA per part (at most the bound;
+        // the CTAs past the number of parts return at once)
+        const int bound = b->ntiles + b->slab_slots;
+        k_tile_parts<<<ceil_div(b->ntiles, TP_WARPS), TP_WARPS * 32, 0, st>>>(
+            b->sys, b->d_tile_prefix, b->nsys, b->ntiles, b->boff, b->tile_parts, b->tp_counter,
+            bound, b->err);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
         if (b->precision == SE_FP32)
-            k_spread2<float><<<b->ntiles, S2_THREADS, 0, st>>>(
+            k_spread2<float><<<bound, S2_THREADS, 0, st>>>(
                 b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
-                static_cast<const float*>(b->rows), b->boff, grid);
+                static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
+                b->tile_done, b->slab, b->slab_slots, b->err);
         else
-            k_spread2<double><<<b->ntiles, S2_THREADS, 0, st>>>(
+            k_spread2<double><<<bound, S2_THREADS, 0, st>>>(
                 b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
-                static_cast<const double*>(b->rows), b->boff, grid);
+                static_cast<const double*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
+                b->tile_done, b->slab, b->slab_slots, b->err);
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
     }

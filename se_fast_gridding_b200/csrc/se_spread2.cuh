@@ -24,7 +24,20 @@
 // packed FP32 pair FMAs on the cells, and after every 512 of the warp's
 // particles the FP32 sums are added into the FP64 grid in place (the first
 // time stored), which the lane alone reads and writes.
+//
+// Crowded tiles are split.  A tile's candidate list (the particles of the
+// bin segments that reach it, in bin order) is cut into parts of at most
+// S2_CAP candidates; k_tile_parts counts each tile's candidates and scans the
+// part counts, and k_spread2 runs one CTA per part.  Part 0 writes the tile
+// into the grid as above; part s >= 1 writes its sums into slab slot
+// (extra parts of the tiles before it) + s - 1, 16^3 FP64 cells; the part
+// that finishes last (a per-tile counter) adds the slabs into the grid in
+// the order s = 1, 2, ...  A tile's parts and their sums depend only on its
+// own candidates, so results stay deterministic and a batched system's grid
+// equals its single solve's.  Uniform inputs at the configurations' densities
+// have far fewer than S2_CAP candidates per tile and are never split.
 
+constexpr int S2_CAP = 8192;   // candidates per part of a tile
 constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
 constexpr int S2_LIST = 64;    // per-warp list ring: >= group - 1 + 32
@@ -158,20 +171,137 @@ __device__ __forceinline__ int tile_half(int g, int ti, int nt, int P)
     return (h == 1 && (g & 15) + P > 16) ? 1 : -1;
 }
 
+// The number of candidates of tile lt of system S (the particles of the bin
+// segments that reach it), summed over the warp; every lane gets it.
+__device__ __forceinline__ int tile_candidates(const SysDev& S, int lt, const int* __restrict__ boff,
+                                               int lane)
+{
+    const int nt = S.nt[0];
+    const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
+    const BinRanges rx = bins_reaching(tix * 16, 16, S.M, S.P, S.nf[0]);
+    const BinRanges ry = bins_reaching(tiy * 16, 16, S.M, S.P, S.nf[1]);
+    const BinRanges rz = bins_reaching(tiz * 16, 16, S.M, S.P, S.nf[2]);
+    const int nx = range_count(rx), ny = range_count(ry);
+    int sum = 0;
+    for (int u = lane; u < nx * ny * 2; u += 32) {
+        const int zr = u & 1, iy = (u >> 1) % ny, ix = (u >> 1) / ny;
+        const int bz0 = zr ? rz.b0 : rz.a0, bz1 = zr ? rz.b1 : rz.a1;
+        if (bz0 <= bz1) {
+            const int kb = S.bin_base + (range_at(rx, ix) * S.nf[1] + range_at(ry, iy)) * S.nf[2];
+            sum += boff[kb + bz1 + 1] - boff[kb + bz0];
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    return sum;
+}
+
+// Parts per tile (one warp per tile: max(1, ceil(candidates / S2_CAP)) for
+// the k_spread2 systems, 1 for the others), then, in the block that finishes
+// last, their exclusive scan in place: parts[t] = the first part of tile t,
+// parts[ntiles] = the number of parts.  More parts than the launch bound
+// (which no input reaches: a bin is a candidate of at most two tiles per
+// axis) set bit 2 of err.  The block counter is left at zero for the next
+// launch.
+constexpr int TP_WARPS = 8;
+
+__global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
+    const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys, int ntiles,
+    const int* __restrict__ boff, int* parts, unsigned* counter, int bound, int* err)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x * TP_WARPS + warp;
+    if (tile < ntiles) {
+        const SysDev& S = sys[find_sys(tile_prefix, nsys, tile)];
+        int n = 1;
+        if (S.path & PATH_TILE_SPREAD) {
+            const int c = tile_candidates(S, tile - S.tile_base, boff, lane);
+            n = max(1, (c + S2_CAP - 1) / S2_CAP);
+        }
+        if (lane == 0) parts[tile] = n;
+    }
+    __shared__ int last;
+    __shared__ int wsum[TP_WARPS];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    int carry = 0;
+    for (int t0 = 0; t0 < ntiles; t0 += TP_WARPS * 32 * 4) {
+        const int idx = t0 + threadIdx.x * 4;
+        int v[4], sum = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            v[i] = idx + i < ntiles ? __ldcg(parts + idx + i) : 0;
+            sum += v[i];
+        }
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        int before = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < TP_WARPS; w++) {
+            before += w < warp ? wsum[w] : 0;
+            tot += wsum[w];
+        }
+        int run = carry + before + incl - sum;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (idx + i < ntiles) parts[idx + i] = run;
+            run += v[i];
+        }
+        carry += tot;
+        __syncthreads();   // wsum is reused
+    }
+    if (threadIdx.x == 0) {
+        parts[ntiles] = carry;
+        if (carry > bound) atomicOr(err, 2);
+        *counter = 0u;
+    }
+}
+
 template <typename Acc>
 __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread2(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
-    const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid)
+    const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid,
+    const int* __restrict__ tile_parts, int ntiles, int* __restrict__ tile_done,
+    double* __restrict__ slab, int slab_slots, int* __restrict__ err)
 {
     constexpr bool FOLD = sizeof(Acc) == 4;
     constexpr int G = s2_group<Acc>();
     constexpr int V = 16 / sizeof(Acc);   // entries per 16-byte copy
     __shared__ __align__(16) Spread2Smem<Acc> sm;
+    __shared__ int folds;   // this CTA finished its tile's parts last
 
-    const int tile = blockIdx.x;
+    // ---- the part this CTA sums: tile = the last t with tile_parts[t] <= item
+    const int item = blockIdx.x;
+    if (item >= tile_parts[ntiles]) return;
+    int tile = 0;
+    {
+        int hi = ntiles - 1;
+        while (tile < hi) {
+            const int mid = (tile + hi + 1) >> 1;
+            if (tile_parts[mid] <= item) tile = mid;
+            else hi = mid - 1;
+        }
+    }
+    const int ipart = item - tile_parts[tile];
+    const int nparts = tile_parts[tile + 1] - tile_parts[tile];
     const SysDev& S = sys[find_sys(tile_prefix, nsys, tile)];
     if (!(S.path & PATH_TILE_SPREAD)) return;   // k_spread covers this system
+    const int slot0 = tile_parts[tile] - tile;   // slab slot of part 1
+    if (ipart > 0 && slot0 + ipart - 1 >= slab_slots) {   // cannot happen: see k_tile_parts
+        if (threadIdx.x == 0) atomicOr(err, 2);
+        return;
+    }
     const int nt = S.nt[0], P = S.P, M = S.M;
     const int lt = tile - S.tile_base;
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
@@ -222,21 +352,28 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
     const unsigned lanes_before = (1u << lane) - 1u;
     int2* list = sm.list[warp];
     double* gs = grid + S.grid_off;
-    const long long plane = (long long)M * M;
+    const long long gplane = (long long)M * M;
+    // part 0 sums into the grid, the others into their slab slot
+    // (cells [x][y][z] of the tile, 16^3)
+    const long long plane = ipart == 0 ? gplane : 256;
     double* cell0 =
-        gs + (long long)x0 * plane + (long long)(y0 + 8 * wy + ly) * M + z0 + 8 * wz + lz;
+        ipart == 0 ? gs + (long long)x0 * gplane + (long long)(y0 + 8 * wy + ly) * M + z0 + 8 * wz + lz
+                  : slab + (long long)(slot0 + ipart - 1) * 4096 + (8 * wy + ly) * 16 + 8 * wz + lz;
+    // this part's candidates: [cbeg, cend) of the tile's list
+    const int cbeg = ipart * S2_CAP, cend = min(total, cbeg + S2_CAP);
 
     Spread2Accum<Acc> acc;
     acc.zero();
-    int cpos = 0, head = 0, tail = 0, buf = 0, pending = 0, since_fold = 0;
+    int cpos = cbeg, head = 0, tail = 0, buf = 0, pending = 0, since_fold = 0;
     int seg = 0;   // the segment holding candidate cpos
+    while (seg + 1 < nseg && sm.seg_pre[seg + 1] <= cpos) seg++;
     bool written = false;
     for (;;) {
         // ---- list at least a group (or every remaining candidate), in order
-        while (tail - head < G && cpos < total) {
+        while (tail - head < G && cpos < cend) {
             const int pos = cpos + lane;
             int part = -1, pk = 0, sl = seg;   // this lane's segment, found forward
-            if (pos < total) {
+            if (pos < cend) {
                 while (sl + 1 < nseg && sm.seg_pre[sl + 1] <= pos) sl++;
                 part = sm.seg_beg[sl] + (pos - sm.seg_pre[sl]);
                 pk = sg[part];
@@ -318,5 +455,26 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread
         if (since_fold > 0 || !written) acc.fold(cell0, plane, !written);
     } else {
         acc.store(cell0, plane);
+    }
+
+    // ---- a split tile: the part that finishes last adds the slabs into the
+    // grid, in part order
+    if (nparts > 1) {
+        __threadfence();
+        __syncthreads();
+        if (t == 0) folds = atomicAdd(&tile_done[tile], 1) == nparts - 1;
+        __syncthreads();
+        if (folds) {
+            __threadfence();
+            for (int c = t; c < 4096; c += S2_THREADS) {
+                const int x = c >> 8, y = (c >> 4) & 15, z = c & 15;
+                double* gp = gs + (long long)(x0 + x) * gplane + (long long)(y0 + y) * M + z0 + z;
+                double v = __ldcg(gp);
+                for (int k = 0; k < nparts - 1; k++)
+                    v += __ldcg(slab + (long long)(slot0 + k) * 4096 + c);
+                *gp = v;
+            }
+            if (t == 0) tile_done[tile] = 0;
+        }
     }
 }

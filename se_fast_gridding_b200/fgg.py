@@ -59,14 +59,31 @@ def fcn_params(M: int, P: int, L: float, xi: float, m: float, N: int) -> tuple[S
     return o, p
 
 
-def pack_params(N, M0, M1, M2, P, c, h, a=None) -> SE_FGG_params:
+def pack_params(N, M0, M1, M2, P, c, h, a=None, b=None) -> SE_FGG_params:
+    """SE_FGG_pack_params; with a, SE2P_FGG_pack_params (z free); with a and
+    b, SE1P_FGG_pack_params (x and y free) -- SE_fgg.c:69-132."""
     p = SE_FGG_params()
     if a is None:
         lib().SE_FGG_pack_params(C.byref(p), N, M0, M1, M2, P, C.c_double(c), C.c_double(h))
-    else:
+    elif b is None:
         lib().SE2P_FGG_pack_params(C.byref(p), N, M0, M1, M2, P, C.c_double(c), C.c_double(h),
                                    C.c_double(a))
+    else:
+        lib().SE1P_FGG_pack_params(C.byref(p), N, M0, M1, M2, P, C.c_double(c), C.c_double(h),
+                                   C.c_double(a), C.c_double(b))
     return p
+
+
+def per_size(p: SE_FGG_params, periodicity: int = 3) -> int:
+    """Elements of the periodic grid SE*_FGG_wrap_fcn writes and
+    SE*_FGG_extend_fcn reads: 3P M0 M1 M2, 2P M0 M1 (M2 + P), 1P the reach of
+    the reference's overlapping column-major map of the padded x, y."""
+    m0, m1, m2 = p.dims
+    if periodicity == 2:
+        return m0 * m1 * p.npdims[2]
+    if periodicity == 1:
+        return (p.npdims[0] - 1) + (p.npdims[1] - 1) * m0 + (m2 - 1) * m0 * m1 + 1
+    return m0 * m1 * m2
 
 
 class Work:

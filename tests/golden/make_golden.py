@@ -200,12 +200,96 @@ def fgg_steps(ref: Ref, ref2p: Ref, x, q, M, P, L, xi, m, tag, out):
     out[f"{tag}/int2p_vanilla"] = phi2
 
 
+def one_periodic_steps(ref1p: Ref, x, q, dims, P, c, tag, out):
+    """The 1P library calls (x and y free with offsets a and b, z periodic):
+    SE1P_FGG_pack_params (SE_fgg.c:113-132), the expansion of a -DONE_PERIODIC
+    build (fgg_expansion_1p, :823-916) through SE_FGG_expand_all, the spread
+    (SE_FGG_grid and SE_FGG_grid_split), SE1P_FGG_wrap_fcn (:387-411),
+    SE1P_FGG_extend_fcn (:478-502) of a seeded field, and the interpolation
+    (SE_FGG_int, SE_FGG_int_split).  The offsets keep every stencil inside
+    the padded grid for positions in [0, 1)."""
+    N = len(q)
+    lib = ref1p.lib
+    M0, M1, M2 = dims
+    h = 1.0 / M2
+    ph = P // 2 if P % 2 == 0 else (P - 1) // 2
+    a, b = -ph * h, -(ph + 0.25) * h
+    p = O.FGGParams()
+    lib.SE1P_FGG_pack_params(C.byref(p), N, M0, M1, M2, P, C.c_double(c), C.c_double(h),
+                             C.c_double(a), C.c_double(b))
+    out[f"{tag}/a"], out[f"{tag}/b"], out[f"{tag}/c"] = np.float64(a), np.float64(b), np.float64(c)
+    out[f"{tag}/dims"] = np.array(dims, dtype=np.int32)
+    out[f"{tag}/d"] = np.float64(p.d)
+    n_pad = int(np.prod(p.npdims))
+    zs = O.aligned_zeros(P ** 3)
+    w = ref1p.work(p, O.aligned_zeros(n_pad), zs, None)
+    lib.SE_FGG_base_gaussian(C.byref(w), C.byref(p))
+    st = O.State()
+    st.x, st.q = O.dptr(x), O.dptr(q)
+    ex = new_exp(N, P, False)
+    w = ref1p.work(p, O.aligned_zeros(n_pad), zs, ex)
+    lib.SE_FGG_expand_all(C.byref(w), C.byref(st), C.byref(p))
+    for k in ("zx", "zy", "zz", "idx"):
+        out[f"{tag}/exp_{k}"] = ex[k].copy()
+    Hv = O.aligned_zeros(n_pad)
+    w = ref1p.work(p, Hv, zs, ex)
+    lib.SE_FGG_grid(C.byref(w), C.byref(st), C.byref(p))
+    put(out, f"{tag}/grid_vanilla", Hv, full=n_pad <= 8000)
+    H = O.aligned_zeros(n_pad)
+    w = ref1p.work(p, H, zs, ex)
+    lib.SE_FGG_grid_split(C.byref(w), C.byref(st), C.byref(p))
+    put(out, f"{tag}/grid_split", H, full=n_pad <= 8000)
+    nper = O.per_size(p, 1)
+    Hper = O.aligned_zeros(nper)
+    lib.SE1P_FGG_wrap_fcn(O.dptr(Hper), C.byref(w), C.byref(p))
+    out[f"{tag}/wrap"] = Hper.copy()
+    rng = np.random.Generator(np.random.Philox(13))
+    F = O.aligned_copy(rng.standard_normal(nper))
+    out[f"{tag}/field"] = F.copy()
+    He = O.aligned_zeros(n_pad)
+    w = ref1p.work(p, He, zs, ex)
+    lib.SE1P_FGG_extend_fcn(C.byref(w), O.dptr(F), C.byref(p))
+    put(out, f"{tag}/extend", He, full=n_pad <= 8000)
+    phi = O.aligned_zeros(N)
+    w = ref1p.work(p, He, zs, ex)
+    lib.SE_FGG_int(O.dptr(phi), C.byref(w), C.byref(st), C.byref(p))
+    out[f"{tag}/int_vanilla"] = phi
+    phi = O.aligned_zeros(N)
+    lib.SE_FGG_int_split(O.dptr(phi), C.byref(w), C.byref(p))
+    out[f"{tag}/int_split"] = phi
+
+
+ONE_P_CASES = [((12, 12, 12), 7), ((12, 12, 12), 8), ((16, 16, 16), 12), ((12, 12, 12), 16),
+               ((20, 20, 20), 21), ((10, 12, 14), 8)]
+
+
+def make_one_periodic(ref_dir):
+    """tests/golden/fgg_1p.npz: the 1P library calls on atoms.txt's first 10
+    atoms rescaled into the unit box."""
+    ref1p = Ref("1p")
+    A = atoms(ref_dir)
+    N, Lb = 10, 3.1814
+    xa = O.aligned_copy(A[:N, :3].T.reshape(-1) / Lb)
+    qa = O.aligned_copy(A[:N, 3])
+    out = {"x": xa, "q": qa, "cases": np.array([list(d) + [P] for d, P in ONE_P_CASES],
+                                                 dtype=np.int32)}
+    for dims, P in ONE_P_CASES:
+        m = 0.95 * np.sqrt(O.PI * P)
+        s = O.Setup(M=dims[2], P=P, L=1.0, xi=4.0, m=m, N=N)
+        c = s.params().c
+        one_periodic_steps(ref1p, xa, qa, dims, P, c, "D{}x{}x{}P{}".format(*dims, P), out)
+    np.savez_compressed(os.path.join(OUT, "fgg_1p.npz"), **out)
+    print("fgg_1p.npz", len(out), "arrays")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("SE_REF_DIR"),
                     help="SE_fast_gridding checkout (default: $SE_REF_DIR)")
     ap.add_argument("--skip-c2", action="store_true")
     ap.add_argument("--realspace-only", action="store_true")
+    ap.add_argument("--one-periodic-only", action="store_true",
+                    help="write tests/golden/fgg_1p.npz only")
     args = ap.parse_args()
     if not args.ref or not os.path.isfile(os.path.join(args.ref, "SE_fgg.c")):
         ap.error("the reference sources are needed: pass --ref <SE_fast_gridding checkout> "
@@ -214,6 +298,8 @@ def main():
                    check=True)
     if args.realspace_only:
         return realspace(Ref("pot"), atoms(args.ref))
+    if args.one_periodic_only:
+        return make_one_periodic(args.ref)
     ref = Ref("pot")
     reff = Ref("force")
     ref2p = Ref("2p")
@@ -300,6 +386,7 @@ def main():
     print("c1.npz: rel-RMS SE vs direct", O.rel_rms(out["phi_ref"], phi_d))
 
     realspace(ref, A)
+    make_one_periodic(args.ref)
     if args.skip_c2:
         return
     # ---------------- 4. C2: FORCE N=1e5, M=128, P=16, xi=20 (1000-particle subset)

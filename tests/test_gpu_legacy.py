@@ -154,6 +154,46 @@ def test_fgg_steps_2p(F, case):
     check_digest(g, f"{tag}/extend2p", w.get("H"), 0.0)
 
 
+ONE_P = [((12, 12, 12), 7), ((12, 12, 12), 8), ((16, 16, 16), 12), ((12, 12, 12), 16),
+         ((20, 20, 20), 21), ((10, 12, 14), 8)]
+
+
+@pytest.mark.parametrize("case", ONE_P)
+def test_fgg_steps_1p(F, case):
+    """SE1P (x and y free, z periodic) against a -DONE_PERIODIC build of the
+    reference: SE1P_FGG_pack_params, the 1P expansion, the split spread,
+    SE1P_FGG_wrap_fcn (whose overlapping column-major map sums in the
+    reference's order: exact), SE1P_FGG_extend_fcn and the interpolation."""
+    g = load_golden("fgg_1p.npz")
+    dims, P = case
+    tag = "D{}x{}x{}P{}".format(*dims, P)
+    x, q = g["x"].copy(), g["q"].copy()
+    M0, M1, M2 = dims
+    p = F.pack_params(10, M0, M1, M2, P, float(g[f"{tag}/c"]), 1.0 / M2, float(g[f"{tag}/a"]),
+                      float(g[f"{tag}/b"]))
+    assert p.d == float(g[f"{tag}/d"])
+    st = F.state(x, q)
+    w = F.Work(p, where="host")
+    F.call("SE_FGG_base_gaussian", C.byref(w.s), C.byref(p))
+    F.call("SE1P_FGG_expand_all", C.byref(w.s), C.byref(st), C.byref(p))
+    np.testing.assert_array_equal(w.get("idx"), g[f"{tag}/exp_idx"])
+    for k in ("zx", "zy", "zz"):
+        np.testing.assert_allclose(w.get(k), g[f"{tag}/exp_{k}"], rtol=1e-13)
+    F.call("SE_FGG_grid_split", C.byref(w.s), C.byref(st), C.byref(p))
+    check_digest(g, f"{tag}/grid_split", w.get("H"), TOL)
+    Hper = np.zeros(F.per_size(p, 1))
+    assert Hper.size == g[f"{tag}/wrap"].size
+    F.call("SE1P_FGG_wrap_fcn", F.dptr(Hper), C.byref(w.s), C.byref(p))
+    np.testing.assert_allclose(Hper, g[f"{tag}/wrap"], rtol=0,
+                               atol=TOL * np.abs(g[f"{tag}/wrap"]).max())
+    field = g[f"{tag}/field"].copy()
+    F.call("SE1P_FGG_extend_fcn", C.byref(w.s), F.dptr(field), C.byref(p))
+    check_digest(g, f"{tag}/extend", w.get("H"), 0.0)
+    phi = np.zeros(10)
+    F.call("SE_FGG_int_split", F.dptr(phi), C.byref(w.s), C.byref(p))
+    np.testing.assert_allclose(phi, g[f"{tag}/int_split"], rtol=TOL)
+
+
 def test_reorder_system(F):
     from test_oracle_golden import reorder_agrees
     g = load_golden("fgg_steps.npz")

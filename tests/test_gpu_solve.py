@@ -207,6 +207,47 @@ def test_spread_tile_aligned_rows_equal_oracle(S, M, P, N, clusters):
     f32.close()
 
 
+@pytest.mark.parametrize("N", [60_000, 8_000])
+def test_spread_split_tiles_equal_oracle(S, N):
+    """Crowded tiles are summed in parts of at most 8192 candidates whose
+    sums are added in part order: at M = 32 every bin is a candidate of every
+    tile, so 60,000 particles split each tile into 8 parts (8,000: one part).
+    FP64 within 1e-12 of the oracle's grid + wrap and full FORCE solve, FP32
+    within its bound, the same bits on a second solve and inside a batch."""
+    import oracle as O
+    M, P = 32, 16
+    x, q = O.synthetic_system(N, 1.0, seed=N, charges="uniform", clusters=1, sigma=0.05)
+    m = S.default_m(P)
+    s = O.Setup(M=M, P=P, L=1.0, xi=6.0, m=m, N=N)
+    p = s.params()
+    Hper = O.wrap(p, O.grid_split(p, q, O.base_gaussian(p), O.expand_all(p, x, 3, False)), 3)
+    ref = Hper.reshape(M, M, M).transpose(2, 1, 0)
+    se = S.SpectralEwald(M, P, 1.0, 6.0, m, "force", "fp64", N)
+    g64 = host(se.spread(cuda(x), cuda(q)))
+    assert rel(g64, ref) < FP64_TOL, rel(g64, ref)
+    s32 = S.SpectralEwald(M, P, 1.0, 6.0, m, "force", "fp32", N)
+    g32 = host(s32.spread(cuda(x), cuda(q)))
+    assert rel(g32, g64) < 5e-7, rel(g32, g64)
+    np.testing.assert_array_equal(host(s32.spread(cuda(x), cuda(q))), g32)
+    f64 = host(se.solve(cuda(x), cuda(q)))
+    fref = O.spectral_ewald(x, q, M, P, m, 1.0, 6.0, "force")
+    assert rel(f64, fref) < FP64_TOL, rel(f64, fref)
+    f32 = host(s32.solve(cuda(x), cuda(q)))
+    assert rel(f32, fref) < FP32_TOL, rel(f32, fref)
+    np.testing.assert_array_equal(host(s32.solve(cuda(x), cuda(q))), f32)
+    # in a batch beside a second (uncrowded) system: the same bits
+    x2, q2 = O.synthetic_system(3000, 2.0, seed=5, charges="uniform")
+    systems = [S.System(N, M, P, 1.0, 6.0, m, "force"), S.System(3000, 48, 12, 2.0, 4.0, None, "force")]
+    for prec, one in (("fp64", f64), ("fp32", f32)):
+        b = S.BatchSolver(systems, precision=prec)
+        xb, qb = b.pack([x, x2], [q, q2])
+        outs = b.split(b.solve(xb, qb))
+        np.testing.assert_array_equal(host(outs[0]), one)
+        b.close()
+    se.close()
+    s32.close()
+
+
 def test_fp32_spread_grid(S):
     import oracle as O
     M, P, N = 64, 12, 20000

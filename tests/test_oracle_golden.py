@@ -82,6 +82,50 @@ def test_fgg_steps_2p(oracle_mod, case):
                                rtol=EXACT)
 
 
+ONE_P = [((12, 12, 12), 7), ((12, 12, 12), 8), ((16, 16, 16), 12), ((12, 12, 12), 16),
+         ((20, 20, 20), 21), ((10, 12, 14), 8)]
+
+
+def one_p_params(O, g, tag):
+    d = g[f"{tag}/dims"]
+    P = int(tag.split("P")[-1])
+    p = O.pack_params(len(g["q"]), int(d[0]), int(d[1]), int(d[2]), P, float(g[f"{tag}/c"]),
+                      1.0 / int(d[2]), float(g[f"{tag}/a"]), float(g[f"{tag}/b"]))
+    return p
+
+
+@pytest.mark.parametrize("case", ONE_P)
+def test_fgg_steps_1p(oracle_mod, case):
+    """SE1P (x and y free, z periodic) against a -DONE_PERIODIC build of the
+    reference: the expansion (fgg_expansion_1p, SE_fgg.c:823-916), spread,
+    SE1P_FGG_wrap_fcn (:387-411, whose column-major map of the padded x, y
+    overlaps itself), SE1P_FGG_extend_fcn (:478-502), interpolation."""
+    O = oracle_mod
+    g = load_golden("fgg_1p.npz")
+    dims, P = case
+    tag = "D{}x{}x{}P{}".format(*dims, P)
+    x, q = g["x"], g["q"]
+    p = one_p_params(O, g, tag)
+    assert p.d == float(g[f"{tag}/d"])
+    zs = O.base_gaussian(p)
+    ex = O.expand_all(p, x, 1, False)
+    np.testing.assert_array_equal(ex["idx"], g[f"{tag}/exp_idx"])
+    for k in ("zx", "zy", "zz"):
+        np.testing.assert_allclose(ex[k], g[f"{tag}/exp_{k}"], rtol=EXACT, atol=0)
+    check_digest(g, f"{tag}/grid_vanilla", O.grid(p, x, q, zs, 1), EXACT)
+    H = O.grid_split(p, q, zs, ex)
+    check_digest(g, f"{tag}/grid_split", H, EXACT)
+    Hper = O.wrap(p, H, 1)
+    assert Hper.size == g[f"{tag}/wrap"].size
+    np.testing.assert_allclose(Hper, g[f"{tag}/wrap"], rtol=0,
+                               atol=EXACT * np.abs(g[f"{tag}/wrap"]).max())
+    He = O.extend(p, g[f"{tag}/field"], 1)
+    check_digest(g, f"{tag}/extend", He, 0.0)
+    np.testing.assert_allclose(O.int_vanilla(p, He, x, zs, 1), g[f"{tag}/int_vanilla"],
+                               rtol=EXACT)
+    np.testing.assert_allclose(O.int_split(p, He, zs, ex), g[f"{tag}/int_split"], rtol=EXACT)
+
+
 @pytest.mark.parametrize("N", [10, 100])
 @pytest.mark.parametrize("P", [8, 12, 16, 21])
 def test_pipeline_matches_reference_spectral_ewald(oracle_mod, N, P):
