@@ -37,7 +37,13 @@
 // equals its single solve's.  Uniform inputs at the configurations' densities
 // have far fewer than S2_CAP candidates per tile and are never split.
 
-constexpr int S2_CAP = 8192;   // candidates per part of a tile
+#ifndef SE_S2_CAP
+#define SE_S2_CAP 8192
+#endif
+#ifndef SE_S2_MIN_BLOCKS
+#define SE_S2_MIN_BLOCKS 4
+#endif
+constexpr int S2_CAP = SE_S2_CAP;   // candidates per part of a tile
 constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
 constexpr int S2_LIST = 64;    // per-warp list ring: >= group - 1 + 32
@@ -268,7 +274,7 @@ __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
 }
 
 template <typename Acc>
-__global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? 4 : 3) k_spread2(
+__global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCKS : 3) k_spread2(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid,
