@@ -892,7 +892,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         if (r != CUFFT_SUCCESS) return fail(cufft_fail(r, "cufftPlanMany"));
     }
     {
-        // the spread tiles want four CTAs of ~48 KB shared memory per SM
+        // the spread tiles want five CTAs of ~37 KB shared memory per SM
         const int carve = (int)cudaSharedmemCarveoutMaxShared;
         cudaError_t a = cudaFuncSetAttribute((const void*)k_spread<float>,
                                              cudaFuncAttributePreferredSharedMemoryCarveout, carve);

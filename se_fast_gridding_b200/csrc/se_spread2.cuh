@@ -41,7 +41,7 @@
 #define SE_S2_CAP 8192
 #endif
 #ifndef SE_S2_MIN_BLOCKS
-#define SE_S2_MIN_BLOCKS 4
+#define SE_S2_MIN_BLOCKS 5
 #endif
 constexpr int S2_CAP = SE_S2_CAP;   // candidates per part of a tile
 constexpr int S2_WARPS = 4;
