@@ -84,6 +84,128 @@ __device__ __forceinline__ void warp_sum4(double& v0, double& v1, double& v2, do
 // z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
 __host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
 
+// The FP32 particle loop: lane l < k P (k = 32 / P groups of P lanes) takes
+// the x row i = l % P of the stencil and, in its group g = l / P, the J =
+// ceil(P / k) y columns j = g J + jj; the lanes past k P repeat group k - 1
+// with zero weights.  A lane's column sums over z (pair loads, packed FMAs
+// against the z weights) combine with its own y weights, held in registers,
+// and its x weight multiplies the lane's sums once, in FP64, before the warp
+// reduction.  Columns past the stencil (j >= P, when k J > P) read the lane's
+// last column with zero weights, so every load stays inside the window and
+// the runtime-P kernel sums in the same order as the P-specialised ones.
+constexpr int I2_JMAX = 8;   // y columns per lane for P <= 16 (k >= 2)
+
+template <int PT, bool FORCE>
+__device__ __forceinline__ void interp2_rows_f32(
+    const SysDev& S, Interp2Warp<float>& W, const float* tile, int P, int o0, int o1, int o2,
+    int pfirst, int pend, const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ sperm, const float* __restrict__ rows, double* __restrict__ out,
+    double* __restrict__ phi_out, int Ep, int PL)
+{
+    using PV = Pair<float>;
+    using VT = float2;
+    const int lane = threadIdx.x & 31;
+    constexpr int NQ = PT ? PT / 2 + 1 : 9;
+    const int nq = P / 2 + 1;
+    constexpr int KC = PT ? 32 / PT : 1;
+    constexpr int JC = PT ? (PT + KC - 1) / KC : I2_JMAX;
+    const int k = PT ? KC : 32 / P;
+    const int J = PT ? JC : (P + k - 1) / k;
+    const int i = lane % P;
+    const int g = min(lane / P, k - 1);
+    const bool active = lane < k * P;
+    // the lane's last column inside the stencil
+    const int jlast = min(J, P - g * J) - 1;
+    for (int p = pfirst; p < pend; p += I2_WARPS) {
+        const double4 rc = srec[p];
+        const int pk = sg[p];
+        const int orig = sperm[p];
+        const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
+        const int r0 = gx - o0, r1 = gy - o1, r2 = gz - o2;
+        const float* rb = rows + (long long)p * 96;
+        W.wz[lane] = 0.f;
+        W.fz[lane] = 0.f;
+        __syncwarp();
+        if (lane < P) {
+            const double off = (S.lo + lane) * S.h;
+            const float vx = rb[(gx & 15) + lane], vy = rb[32 + (gy & 15) + lane],
+                        vz = rb[64 + (gz & 15) + lane];
+            W.wx[lane] = vx;
+            W.wy[lane] = vy;
+            W.wz[r2 + lane] = vz;
+            if (FORCE) {
+                W.fx[lane] = (float)((double)vx * (-S.c * (rc.x - off)));
+                W.fy[lane] = (float)((double)vy * (-S.c * (rc.y - off)));
+                W.fz[r2 + lane] = (float)((double)vz * (-S.c * (rc.z - off)));
+            }
+        }
+        __syncwarp();
+        const int q0 = r2 >> 1;
+        VT wz2[NQ], fz2[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            if (PT || q < nq) {
+                wz2[q] = PV::load(W.wz + 2 * (q0 + q));
+                fz2[q] = FORCE ? PV::load(W.fz + 2 * (q0 + q)) : PV::zero();
+            }
+        }
+        const float wxi = active ? W.wx[i] : 0.f;
+        const float fxi = (FORCE && active) ? W.fx[i] : 0.f;
+        float wy[JC], fy[JC];
+#pragma unroll
+        for (int jj = 0; jj < JC; jj++) {
+            const bool ok = jj < J && jj <= jlast;
+            wy[jj] = ok ? W.wy[g * J + jj] : 0.f;
+            fy[jj] = (FORCE && ok) ? W.fy[g * J + jj] : 0.f;
+        }
+        const float* col = tile + (r0 + i) * PL + (r1 + g * J) * Ep + 2 * q0;
+        float a_pot = 0.f, a_fy = 0.f, a_fz = 0.f;
+        auto columns = [&](auto nqc) {
+            constexpr int NQC = decltype(nqc)::value;
+#pragma unroll
+            for (int jj = 0; jj < JC; jj++) {
+                if (!PT && jj >= J) break;
+                const float* cj = col + (PT && KC * JC == PT ? jj : min(jj, jlast)) * Ep;
+                VT s0 = PV::zero(), s1 = PV::zero();
+#pragma unroll
+                for (int q = 0; q < NQC; q++) {
+                    if (PT || q < nq) {
+                        const VT g2 = PV::load(cj + 2 * q);
+                        s0 = PV::fma(g2, wz2[q], s0);
+                        if (FORCE) s1 = PV::fma(g2, fz2[q], s1);
+                    }
+                }
+                const float t0 = PV::sum(s0);
+                a_pot = fmaf(t0, wy[jj], a_pot);
+                if (FORCE) {
+                    a_fy = fmaf(t0, fy[jj], a_fy);
+                    a_fz = fmaf(PV::sum(s1), wy[jj], a_fz);
+                }
+            }
+        };
+        // an even stencil that starts on a pair spans P/2 pairs, not P/2 + 1
+        // (a warp-uniform choice: the pair the other form adds is zero)
+        if (PT != 0 && PT % 2 == 0 && (r2 & 1) == 0)
+            columns(std::integral_constant<int, (PT ? PT / 2 : 1)>{});
+        else
+            columns(std::integral_constant<int, NQ>{});
+        double d_pot = (double)a_pot * (double)wxi;
+        double d_fx = 0, d_fy = 0, d_fz = 0;
+        if (FORCE) {
+            d_fx = (double)a_pot * (double)fxi;
+            d_fy = (double)a_fy * (double)wxi;
+            d_fz = (double)a_fz * (double)wxi;
+            warp_sum4(d_pot, d_fx, d_fy, d_fz);
+        } else {
+            d_pot = warp_sum(d_pot);
+        }
+        if (lane == 0)
+            interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz,
+                         S.mode == SE_FORCE, out, phi_out);
+        __syncwarp();
+    }
+}
+
 // FORCE: the force weights and sums are computed (every system of a batch
 // with a FORCE system runs this variant; each stores what its mode asks).
 template <typename T, int PT, bool FORCE>
@@ -145,6 +267,12 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     constexpr bool force = FORCE;
     constexpr int NQ = PT ? PT / 2 + 1 : 9;   // z pairs a stencil spans (<= 9 for P <= 16)
     const int nq = P / 2 + 1;
+    if constexpr (sizeof(T) == 4) {
+        interp2_rows_f32<PT, FORCE>(S, wsm[warp], reinterpret_cast<const float*>(tile), P, o0,
+                                    o1, o2, beg + warp, end, srec, sg, sperm,
+                                    reinterpret_cast<const float*>(rows), out, phi_out, Ep, PL);
+        return;
+    }
     const bool JFIX = (32 % P) == 0;
     for (int p = beg + warp; p < end; p += I2_WARPS) {
         const double4 rc = srec[p];

@@ -647,29 +647,46 @@ static cudaError_t raise_smem_limit(const void* fn, size_t smem)
 }
 
 // Row pitch Ep and plane pitch PL (elements, both even) of k_interp2's
-// window for stencils up to P: the pair loads of one warp instruction (lane
-// l reads column c = l + 32 m, i = c / P, j = c % P) are served in 128-byte
-// groups of lanes; count, over all rounds m, the largest number of distinct
-// 4-byte words that share a bank within a group, and keep the smallest.
+// window for stencils up to P: the pair loads of one warp instruction are
+// served in 128-byte groups of lanes; count, over all load rounds m, the
+// largest number of distinct 4-byte words that share a bank within a group,
+// and keep the smallest.
 static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
 {
     const int E = FB + P - 1, EZ = interp2_ez(P);
     const int words = precision == SE_FP32 ? 2 : 4;   // 4-byte words per pair
     const int group = 32 / words;                     // lanes per 128 bytes
+    // the lanes' (x, y) columns per load round: FP32 (interp2_rows_f32) lane
+    // l takes row i = l % P and the columns j = g J + m of its group g; FP64
+    // lane l takes column c = l + 32 m, i = c / P, j = c % P
+    const int k = 32 / P, J = (P + k - 1) / k;
+    const int rounds = precision == SE_FP32 ? J : (P * P + 31) / 32;
+    auto column = [&](int l, int m, int* i, int* j) {
+        if (precision == SE_FP32) {
+            const int g = std::min(l / P, k - 1);
+            *i = l % P;
+            *j = g * J + std::min(m, std::min(J, P - g * J) - 1);
+            return true;
+        }
+        const int c = l + 32 * m;
+        *i = c / P;
+        *j = c % P;
+        return c < P * P;
+    };
     int best_cost = 1 << 30, best_Ep = EZ, best_PL = E * EZ;
     for (int Ep = EZ; Ep <= EZ + 32; Ep += 2) {
         for (int pad = 0; pad <= 64; pad += 2) {
             const int PL = E * Ep + pad;
             int cost = 0;
-            for (int m = 0; m * 32 < P * P; m++) {
+            for (int m = 0; m < rounds; m++) {
                 for (int g0 = 0; g0 < 32; g0 += group) {
                     int wordsat[32][8];
                     int nw[32] = {0};
                     int worst = 0;
                     for (int l = g0; l < g0 + group; l++) {
-                        const int c = l + 32 * m;
-                        if (c >= P * P) continue;
-                        const int e = (c / P) * PL + (c % P) * Ep;   // element offset
+                        int ci, cj;
+                        if (!column(l, m, &ci, &cj)) continue;
+                        const int e = ci * PL + cj * Ep;   // element offset
                         for (int w = 0; w < words; w++) {
                             const int word = e * (words / 2) + w, bank = word & 31;
                             bool seen = false;

@@ -43,6 +43,9 @@
 #ifndef SE_S2_MIN_BLOCKS
 #define SE_S2_MIN_BLOCKS 5
 #endif
+#ifndef SE_S2_FULL_GROUP
+#define SE_S2_FULL_GROUP 1
+#endif
 constexpr int S2_CAP = SE_S2_CAP;   // candidates per part of a tile
 constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
@@ -419,6 +422,15 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
                 }
                 cp_async8(&st.q[lane], &srec[e.x].w);
             }
+#if SE_S2_FULL_GROUP
+            else {   // a short (the last) group: zero rows, so every group sums G rows
+#pragma unroll
+                for (int k = 0; k < 16; k++) st.px[lane][k] = Acc(0);
+#pragma unroll
+                for (int k = 0; k < 8; k++) st.py[lane][k] = st.pz[lane][k] = Acc(0);
+                st.q[lane] = 0.0;
+            }
+#endif
             cp_async_commit();
             head += n;
         }
@@ -436,8 +448,15 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
                 for (int k = 0; k < 8; k++) st.py[lane][k] = st.py[lane][k] * qv;
             }
             __syncwarp();
+#if SE_S2_FULL_GROUP
+            // every group holds G rows (a short one padded with zeros, which
+            // add exact zeros): one unrolled pass with constant offsets
+#pragma unroll
+            for (int i = 0; i < G; i++) {
+#else
 #pragma unroll 2
             for (int i = 0; i < pending; i++) {
+#endif
                 const Acc y = st.py[i][ly];
                 acc.add(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
             }
