@@ -656,13 +656,15 @@ static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
     const int E = FB + P - 1, EZ = interp2_ez(P);
     const int words = precision == SE_FP32 ? 2 : 4;   // 4-byte words per pair
     const int group = 32 / words;                     // lanes per 128 bytes
-    // the lanes' (x, y) columns per load round: FP32 (interp2_rows_f32) lane
-    // l takes row i = l % P and the columns j = g J + m of its group g; FP64
-    // lane l takes column c = l + 32 m, i = c / P, j = c % P
+    // the lanes' (x, y) columns per load round: FP32 with P not dividing 32
+    // (interp2_rows_f32) lane l takes row i = l % P and the columns
+    // j = g J + m of its group g; otherwise lane l takes column c = l + 32 m,
+    // i = c / P, j = c % P
     const int k = 32 / P, J = (P + k - 1) / k;
-    const int rounds = precision == SE_FP32 ? J : (P * P + 31) / 32;
+    const bool rows_map = precision == SE_FP32 && 32 % P != 0;
+    const int rounds = rows_map ? J : (P * P + 31) / 32;
     auto column = [&](int l, int m, int* i, int* j) {
-        if (precision == SE_FP32) {
+        if (rows_map) {
             const int g = std::min(l / P, k - 1);
             *i = l % P;
             *j = g * J + std::min(m, std::min(J, P - g * J) - 1);

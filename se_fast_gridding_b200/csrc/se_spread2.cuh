@@ -423,7 +423,8 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
                 cp_async8(&st.q[lane], &srec[e.x].w);
             }
 #if SE_S2_FULL_GROUP
-            else {   // a short (the last) group: zero rows, so every group sums G rows
+            else if (lane < G) {   // a short (the last) group: zero rows up to G (FP64: 16),
+                                   // so every group sums G rows
 #pragma unroll
                 for (int k = 0; k < 16; k++) st.px[lane][k] = Acc(0);
 #pragma unroll
