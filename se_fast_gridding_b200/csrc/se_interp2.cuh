@@ -84,6 +84,54 @@ __device__ __forceinline__ void warp_sum4(double& v0, double& v1, double& v2, do
 // z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
 __host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
 
+// FP32: the next particle's record, packed corner, input index and factor
+// rows, copied by cp.async into a per-warp slot while the warp sums the
+// current particle (two slots, alternating), so the global-load latency of
+// each particle's data is not waited for.
+#ifndef SE_I2_PREFETCH
+#define SE_I2_PREFETCH 1
+#endif
+#ifndef SE_I2_ASYNC_STAGE
+#define SE_I2_ASYNC_STAGE 1
+#endif
+
+struct __align__(16) Interp2Next {
+    float rows[2][96];
+    double4 rec[2];
+    int pk[2], orig[2];
+};
+
+__device__ __forceinline__ Interp2Next* interp2_next_slots()
+{
+    __shared__ Interp2Next slots[I2_WARPS];
+    return slots;
+}
+
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+
+// Lanes 0-23 copy the 384-byte factor rows of particle p, 24-25 its record,
+// 26 its corner, 27 its input index into slot `slot`.
+__device__ __forceinline__ void interp2_fetch(Interp2Next& nx, int slot, int p,
+                                              const double4* __restrict__ srec,
+                                              const int* __restrict__ sg,
+                                              const int* __restrict__ sperm,
+                                              const float* __restrict__ rows, int lane)
+{
+    if (lane < 24)
+        cp_async16(&nx.rows[slot][4 * lane], rows + (long long)p * 96 + 4 * lane);
+    else if (lane < 26)
+        cp_async16(reinterpret_cast<char*>(&nx.rec[slot]) + 16 * (lane - 24),
+                   reinterpret_cast<const char*>(srec + p) + 16 * (lane - 24));
+    else if (lane == 26)
+        cp_async4(&nx.pk[slot], sg + p);
+    else if (lane == 27)
+        cp_async4(&nx.orig[slot], sperm + p);
+}
+
 // The FP32 particle loop for P that does not divide 32 (P = 12 among the
 // configurations; P = 8 and 16 take the column mapping of k_interp2, which
 // measured 17% and 2% faster there): lane l < k P (k = 32 / P groups of P lanes) takes
@@ -118,13 +166,34 @@ __device__ __forceinline__ void interp2_rows_f32(
     const bool active = lane < k * P;
     // the lane's last column inside the stencil
     const int jlast = min(J, P - g * J) - 1;
-    for (int p = pfirst; p < pend; p += I2_WARPS) {
-        const double4 rc = srec[p];
-        const int pk = sg[p];
-        const int orig = sperm[p];
+    Interp2Next& nx = interp2_next_slots()[threadIdx.x >> 5];
+    if (SE_I2_PREFETCH) {
+        if (pfirst < pend) interp2_fetch(nx, 0, pfirst, srec, sg, sperm, rows, lane);
+        cp_async_commit();
+    }
+    int slot = 0;
+    for (int p = pfirst; p < pend; p += I2_WARPS, slot ^= 1) {
+        double4 rc;
+        int pk, orig;
+        const float* rb;
+        if (SE_I2_PREFETCH) {
+            if (p + I2_WARPS < pend)
+                interp2_fetch(nx, slot ^ 1, p + I2_WARPS, srec, sg, sperm, rows, lane);
+            cp_async_commit();
+            cp_async_wait<1>();
+            __syncwarp();
+            rc = nx.rec[slot];
+            pk = nx.pk[slot];
+            orig = nx.orig[slot];
+            rb = nx.rows[slot];
+        } else {
+            rc = srec[p];
+            pk = sg[p];
+            orig = sperm[p];
+            rb = rows + (long long)p * 96;
+        }
         const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
         const int r0 = gx - o0, r1 = gy - o1, r2 = gz - o2;
-        const float* rb = rows + (long long)p * 96;
         W.wz[lane] = 0.f;
         W.fz[lane] = 0.f;
         __syncwarp();
@@ -204,8 +273,9 @@ __device__ __forceinline__ void interp2_rows_f32(
         if (lane == 0)
             interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz,
                          S.mode == SE_FORCE, out, phi_out);
-        __syncwarp();
+        __syncwarp();   // the slot is read before it is refilled
     }
+    if (SE_I2_PREFETCH) cp_async_wait<0>();
 }
 
 // FORCE: the force weights and sums are computed (every system of a batch
@@ -251,6 +321,17 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
             z -= z >= M ? M : 0;
             const T* src = gs + ((long long)x * M + y) * M + z;
             T* dst = tile + a * PL + b * Ep + g * G;
+#if SE_I2_ASYNC_STAGE
+            // straight into shared memory: two copies of a cell pair each
+            // (the window's rows are 8-byte aligned in FP32, 16 in FP64)
+            if constexpr (sizeof(T) == 4) {
+                cp_async8(dst, src);
+                cp_async8(dst + 2, src + 2);
+            } else {
+                cp_async16(dst, src);
+                cp_async16(dst + 2, src + 2);
+            }
+#else
             if constexpr (sizeof(T) == 4) {
                 const float4 v = __ldg(reinterpret_cast<const float4*>(src));
                 reinterpret_cast<float2*>(dst)[0] = make_float2(v.x, v.y);
@@ -261,8 +342,13 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
                 reinterpret_cast<double2*>(dst)[0] = v0;
                 reinterpret_cast<double2*>(dst)[1] = v1;
             }
+#endif
         }
     }
+#if SE_I2_ASYNC_STAGE
+    cp_async_commit();
+    cp_async_wait<0>();
+#endif
     __syncthreads();
 
     Interp2Warp<T>& W = wsm[warp];
@@ -283,14 +369,39 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
             return;
         }
     }
-    for (int p = beg + warp; p < end; p += I2_WARPS) {
-        const double4 rc = srec[p];
-        const int pk = sg[p];
-        const int orig = sperm[p];
+    constexpr bool PF = sizeof(T) == 4 && SE_I2_PREFETCH;
+    Interp2Next* nx = nullptr;
+    if constexpr (PF) {
+        nx = interp2_next_slots() + warp;
+        if (beg + warp < end)
+            interp2_fetch(*nx, 0, beg + warp, srec, sg, sperm,
+                          reinterpret_cast<const float*>(rows), lane);
+        cp_async_commit();
+    }
+    int slot = 0;
+    for (int p = beg + warp; p < end; p += I2_WARPS, slot ^= 1) {
+        double4 rc;
+        int pk, orig;
+        const T* rb;   // weights: lane i < P holds factor i of each axis (tile-aligned rows)
+        if constexpr (PF) {
+            if (p + I2_WARPS < end)
+                interp2_fetch(*nx, slot ^ 1, p + I2_WARPS, srec, sg, sperm,
+                              reinterpret_cast<const float*>(rows), lane);
+            cp_async_commit();
+            cp_async_wait<1>();
+            __syncwarp();
+            rc = nx->rec[slot];
+            pk = nx->pk[slot];
+            orig = nx->orig[slot];
+            rb = reinterpret_cast<const T*>(nx->rows[slot]);
+        } else {
+            rc = srec[p];
+            pk = sg[p];
+            orig = sperm[p];
+            rb = rows + (long long)p * 96;
+        }
         const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
         const int r0 = gx - o0, r1 = gy - o1, r2 = gz - o2;
-        // weights: lane i < P holds factor i of each axis (tile-aligned rows)
-        const T* rb = rows + (long long)p * 96;
         W.wz[lane] = T(0);
         W.fz[lane] = T(0);
         __syncwarp();
@@ -383,8 +494,9 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
         if (lane == 0)
             interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz,
                          S.mode == SE_FORCE, out, phi_out);
-        __syncwarp();
+        __syncwarp();   // (FP32) the slot is read before it is refilled
     }
+    if constexpr (PF) cp_async_wait<0>();
 }
 
 // Every FP64 grid value of the batch as FP32 (the staged source of
