@@ -6,16 +6,19 @@
 //
 // One CTA per fine bin (8^3 stencil corners).  The bin's window, E = 7 + P
 // cells per axis in x and y and EZ = 8 + P rounded up to 4 in z, is copied
-// from the grid (a FP32 copy of it on the FP32 path) with 16-byte loads: the
-// window starts on a multiple of 8 in every axis and M is a multiple of 16,
-// so every 4-cell group is contiguous even where the window wraps.  One warp
-// per particle; lane l takes the (x, y) columns l, l + 32, ... and sums each
-// column over z in pairs: one 8-byte (FP32) or 16-byte (FP64) shared load of
-// two neighbouring cells feeds two packed FMAs per accumulator against the
-// particle's z weights, which are zero-padded pairs in registers aligned to
-// the window.  Columns combine with the x (and y) weights in the working
-// precision; the lanes' sums are reduced in FP64 with shuffles (the four
-// FORCE sums of the FP32 kernel together, warp_sum4).
+// from the grid (a FP32 copy of it on the FP32 path) by cp.async, a 4-cell
+// group at a time: the window starts on a multiple of 8 in every axis and M
+// is a multiple of 16, so every group is contiguous even where the window
+// wraps.  One warp per particle; lane l takes the (x, y) columns l, l + 32,
+// ... (FP32 with P not dividing 32: a whole x row, interp2_rows_f32) and
+// sums each column over z in pairs: one 8-byte (FP32) or 16-byte (FP64)
+// shared load of two neighbouring cells feeds two packed FMAs per
+// accumulator against the particle's z weights, which are zero-padded pairs
+// in registers aligned to the window.  Columns combine with the x (and y)
+// weights in the working precision; the lanes' sums are reduced in FP64 with
+// shuffles (the four FORCE sums of the FP32 kernel together, warp_sum4).
+// FP32 warps copy the next particle's record and factor rows into shared
+// memory by cp.async while they sum the current one.
 //
 // Shared-memory pitches (row Ep, plane PL) come from the host, chosen so that
 // the pair loads of one instruction fall in distinct banks.
