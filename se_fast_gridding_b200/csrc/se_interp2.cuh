@@ -17,8 +17,8 @@
 // in registers aligned to the window.  Columns combine with the x (and y)
 // weights in the working precision; the lanes' sums are reduced in FP64 with
 // shuffles (the four FORCE sums of the FP32 kernel together, warp_sum4).
-// FP32 warps copy the next particle's record and factor rows into shared
-// memory by cp.async while they sum the current one.
+// FP32 warps on x rows copy the next particle's record and factor rows into
+// shared memory by cp.async while they sum the current one.
 //
 // Shared-memory pitches (row Ep, plane PL) come from the host, chosen so that
 // the pair loads of one instruction fall in distinct banks.
@@ -87,10 +87,12 @@ __device__ __forceinline__ void warp_sum4(double& v0, double& v1, double& v2, do
 // z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
 __host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
 
-// FP32: the next particle's record, packed corner, input index and factor
-// rows, copied by cp.async into a per-warp slot while the warp sums the
-// current particle (two slots, alternating), so the global-load latency of
-// each particle's data is not waited for.
+// FP32 rows of x (interp2_rows_f32): the next particle's record, packed
+// corner, input index and factor rows, copied by cp.async into a per-warp
+// slot while the warp sums the current particle (two slots, alternating), so
+// the global-load latency of each particle's data is not waited for.  (The
+// column mapping of P = 8 and 16 measured 8% and 1.5% slower with it, P = 12
+// 3% faster.)
 #ifndef SE_I2_PREFETCH
 #define SE_I2_PREFETCH 1
 #endif
@@ -372,39 +374,14 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
             return;
         }
     }
-    constexpr bool PF = sizeof(T) == 4 && SE_I2_PREFETCH;
-    Interp2Next* nx = nullptr;
-    if constexpr (PF) {
-        nx = interp2_next_slots() + warp;
-        if (beg + warp < end)
-            interp2_fetch(*nx, 0, beg + warp, srec, sg, sperm,
-                          reinterpret_cast<const float*>(rows), lane);
-        cp_async_commit();
-    }
-    int slot = 0;
-    for (int p = beg + warp; p < end; p += I2_WARPS, slot ^= 1) {
-        double4 rc;
-        int pk, orig;
-        const T* rb;   // weights: lane i < P holds factor i of each axis (tile-aligned rows)
-        if constexpr (PF) {
-            if (p + I2_WARPS < end)
-                interp2_fetch(*nx, slot ^ 1, p + I2_WARPS, srec, sg, sperm,
-                              reinterpret_cast<const float*>(rows), lane);
-            cp_async_commit();
-            cp_async_wait<1>();
-            __syncwarp();
-            rc = nx->rec[slot];
-            pk = nx->pk[slot];
-            orig = nx->orig[slot];
-            rb = reinterpret_cast<const T*>(nx->rows[slot]);
-        } else {
-            rc = srec[p];
-            pk = sg[p];
-            orig = sperm[p];
-            rb = rows + (long long)p * 96;
-        }
+    for (int p = beg + warp; p < end; p += I2_WARPS) {
+        const double4 rc = srec[p];
+        const int pk = sg[p];
+        const int orig = sperm[p];
         const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
         const int r0 = gx - o0, r1 = gy - o1, r2 = gz - o2;
+        // weights: lane i < P holds factor i of each axis (tile-aligned rows)
+        const T* rb = rows + (long long)p * 96;
         W.wz[lane] = T(0);
         W.fz[lane] = T(0);
         __syncwarp();
@@ -497,9 +474,8 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
         if (lane == 0)
             interp_store(S, orig - S.part_off, rc.w, d_pot, d_fx, d_fy, d_fz,
                          S.mode == SE_FORCE, out, phi_out);
-        __syncwarp();   // (FP32) the slot is read before it is refilled
+        __syncwarp();
     }
-    if constexpr (PF) cp_async_wait<0>();
 }
 
 // Every FP64 grid value of the batch as FP32 (the staged source of
