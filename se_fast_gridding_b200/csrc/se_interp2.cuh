@@ -283,6 +283,13 @@ __device__ __forceinline__ void interp2_rows_f32(
     if (SE_I2_PREFETCH) cp_async_wait<0>();
 }
 
+template <typename T, int PT, bool FORCE>
+__device__ __forceinline__ void interp2_columns(
+    const SysDev& S, Interp2Warp<T>& W, const T* tile, int P, int o0, int o1, int o2,
+    int pfirst, int pend, const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ sperm, const T* __restrict__ rows, double* __restrict__ out,
+    double* __restrict__ phi_out, int Ep, int PL, bool JFIX);
+
 // FORCE: the force weights and sums are computed (every system of a batch
 // with a FORCE system runs this variant; each stores what its mode asks).
 template <typename T, int PT, bool FORCE>
@@ -311,7 +318,7 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     const int E = FB + P - 1, EZ = interp2_ez(P);
     T* tile = reinterpret_cast<T*>(dsm);
     const T* gs = grid + S.grid_off;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
 
     // ---- stage the window: rows (a, b), groups of 4 cells along z
     {
@@ -357,9 +364,6 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     __syncthreads();
 
     Interp2Warp<T>& W = wsm[warp];
-    constexpr bool force = FORCE;
-    constexpr int NQ = PT ? PT / 2 + 1 : 9;   // z pairs a stencil spans (<= 9 for P <= 16)
-    const int nq = P / 2 + 1;
     const bool JFIX = (32 % P) == 0;
     if constexpr (sizeof(T) == 4) {
         // stencils whose P does not divide 32 (P = 12): x rows per lane; the
@@ -371,10 +375,29 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
                                         o0, o1, o2, beg + warp, end, srec, sg, sperm,
                                         reinterpret_cast<const float*>(rows), out, phi_out, Ep,
                                         PL);
-            return;
         }
     }
-    for (int p = beg + warp; p < end; p += I2_WARPS) {
+    if (sizeof(T) == 4 && !JFIX) return;
+    interp2_columns<T, PT, FORCE>(S, W, tile, P, o0, o1, o2, beg + warp, end, srec, sg, sperm,
+                                  rows, out, phi_out, Ep, PL, JFIX);
+}
+
+// The column mapping (FP64, and FP32 with P dividing 32): lane l takes the
+// (x, y) columns c = l, l + 32, ..., i = c / P, j = c % P.
+template <typename T, int PT, bool FORCE>
+__device__ __forceinline__ void interp2_columns(
+    const SysDev& S, Interp2Warp<T>& W, const T* tile, int P, int o0, int o1, int o2,
+    int pfirst, int pend, const double4* __restrict__ srec, const int* __restrict__ sg,
+    const int* __restrict__ sperm, const T* __restrict__ rows, double* __restrict__ out,
+    double* __restrict__ phi_out, int Ep, int PL, bool JFIX)
+{
+    using PV = Pair<T>;
+    using VT = typename PV::V;
+    const int lane = threadIdx.x & 31;
+    constexpr bool force = FORCE;
+    constexpr int NQ = PT ? PT / 2 + 1 : 9;   // z pairs a stencil spans (<= 9 for P <= 16)
+    const int nq = P / 2 + 1;
+    for (int p = pfirst; p < pend; p += I2_WARPS) {
         const double4 rc = srec[p];
         const int pk = sg[p];
         const int orig = sperm[p];
