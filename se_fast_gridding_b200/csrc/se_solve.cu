@@ -224,16 +224,16 @@ __device__ __forceinline__ double kwave(int i, int M, double kfac)
 // spec *= Z on the half spectrum [x][y][z <= M/2]; Z = exp(scalar K2)/K2 * 4pi/M^3
 // with K2 summed in the reference's order (its first FFT axis is our z).
 //
-// One block takes SCALE_ROWS (x, y) rows of one system.  The grid is cubic, so
-// k^2 and exp(scalar k^2) of the M wave numbers of one axis go into a shared
-// table first, and exp(scalar K2) is the product of three table entries (a
-// few ulps from the exponential of the sum, far inside the FP64 tolerance);
-// the row's x and y entries are read once per row.  The block's threads take
-// z < Mh - 1 of each row (Mh = M/2 + 1), then the rows' last z together.
-constexpr int SCALE_ROWS = 32;
+// One block of SCALE_THREADS takes SCALE_ROWS (x, y) rows of one system.  The
+// grid is cubic, so k^2 and exp(scalar k^2) of the M wave numbers of one axis
+// go into a shared table first, and exp(scalar K2) is the product of three
+// table entries (a few ulps from the exponential of the sum, far inside the
+// FP64 tolerance).  The threads form rows_per_pass groups of TZ = M/2 rounded
+// up to a warp (at most SCALE_THREADS): a group takes z < Mh - 1 of one row
+// (Mh = M/2 + 1) while the other groups take the next rows, and the rows'
+// last z go one per thread at the end.
+constexpr int SCALE_ROWS = 32, SCALE_THREADS = 256;
 
-// threads per block of the Z pass for grids up to M
-inline int scale_threads(int M) { return std::min(256, std::max(32, (M / 2 + 31) / 32 * 32)); }
 
 template <typename V>
 __device__ __forceinline__ void scale_by(V& v, double Z);
@@ -256,15 +256,16 @@ __device__ __forceinline__ void scale_by<float2>(float2& v, double Z)
 // blockIdx.y] (order NULL: system blockIdx.y); dynamic shared memory of
 // 2 M doubles for the largest M launched.
 template <typename V>
-__global__ void k_scale_rows(const SysDev* __restrict__ sys, const int* __restrict__ order,
-                             int first, V* __restrict__ spec)
+__global__ void __launch_bounds__(SCALE_THREADS) k_scale_rows(const SysDev* __restrict__ sys,
+                                                              const int* __restrict__ order,
+                                                              int first, V* __restrict__ spec)
 {
     extern __shared__ double ktab[];   // [0, M): k^2; [M, 2M): exp(scalar k^2)
     const SysDev& S = sys[order ? order[first + blockIdx.y] : blockIdx.y];
     const int M = S.M, Mh = M / 2 + 1;
     const int r0 = blockIdx.x * SCALE_ROWS;
     if (r0 >= M * M) return;   // a smaller grid than the launch's largest
-    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+    for (int i = threadIdx.x; i < M; i += SCALE_THREADS) {
         const double k = kwave(i, M, S.kfac);
         const double k2 = k * k;
         ktab[i] = k2;
@@ -273,6 +274,8 @@ __global__ void k_scale_rows(const SysDev* __restrict__ sys, const int* __restri
     __syncthreads();
     V* sp = spec + S.spec_off;
     const int nrow = min(SCALE_ROWS, M * M - r0);
+    const int tz = min(SCALE_THREADS, max(32, (M / 2 + 31) / 32 * 32));
+    const int rpp = SCALE_THREADS / tz;   // rows per pass
     auto one = [&](int r, int iz) {
         const int ix = r / M, iy = r - ix * M;
         const long long e = (long long)r * Mh + iz;
@@ -283,9 +286,11 @@ __global__ void k_scale_rows(const SysDev* __restrict__ sys, const int* __restri
         scale_by(v, Z);
         sp[e] = v;
     };
-    for (int rr = 0; rr < nrow; rr++)
-        for (int iz = threadIdx.x; iz < Mh - 1; iz += blockDim.x) one(r0 + rr, iz);
-    for (int rr = threadIdx.x; rr < nrow; rr += blockDim.x) one(r0 + rr, Mh - 1);
+    const int sub = threadIdx.x / tz, z0 = threadIdx.x - sub * tz;
+    if (sub < rpp)
+        for (int rr = sub; rr < nrow; rr += rpp)
+            for (int iz = z0; iz < Mh - 1; iz += tz) one(r0 + rr, iz);
+    for (int rr = threadIdx.x; rr < nrow; rr += SCALE_THREADS) one(r0 + rr, Mh - 1);
 }
 
 #include "se_fft.cuh"
@@ -1073,7 +1078,7 @@ static int run_kspace32(se_batch b, const double* grid, cudaStream_t st)
     for (auto& g : b->groups) maxM = std::max(maxM, g.M);
     const dim3 gs(ceil_div((long)maxM * maxM, SCALE_ROWS), b->nsys);
     SE_CUDA(raise_smem_limit((const void*)k_scale_rows<float2>, 16 * (size_t)maxM));
-    k_scale_rows<float2><<<gs, scale_threads(maxM), 16 * (size_t)maxM, st>>>(b->sys, nullptr, 0,
+    k_scale_rows<float2><<<gs, SCALE_THREADS, 16 * (size_t)maxM, st>>>(b->sys, nullptr, 0,
                                                                              b->spec32);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
@@ -1128,7 +1133,7 @@ static int run_kspace(se_batch b, double* grid, cudaStream_t st, bool* grid32_fr
                               reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off)));
         const dim3 gs(ceil_div((long)g.M * g.M, SCALE_ROWS), g.count);
         SE_CUDA(raise_smem_limit((const void*)k_scale_rows<double2>, 16 * (size_t)g.M));
-        k_scale_rows<double2><<<gs, scale_threads(g.M), 16 * (size_t)g.M, st>>>(
+        k_scale_rows<double2><<<gs, SCALE_THREADS, 16 * (size_t)g.M, st>>>(
             b->sys, b->d_order, g.first, b->spec);
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
