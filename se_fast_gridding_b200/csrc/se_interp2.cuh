@@ -435,34 +435,63 @@ __device__ __forceinline__ void interp2_columns(
         // the columns, summing NQC z pairs each
         auto columns = [&](auto nqc) {
             constexpr int NQC = decltype(nqc)::value;
-            for (int c = lane; c < P * P; c += 32) {
-                const int i = c / P, j = c - (c / P) * P;
-                const T* col = tile + (r0 + i) * PL + (r1 + j) * Ep + 2 * q0;
-                VT s0 = PV::zero(), s1 = PV::zero();
+            if constexpr (PT != 0 && 32 % PT == 0) {
+                // P divides 32: lane l's columns are rows i = l / P + m (32 / P)
+                // of the fixed column j = l % P, m < P^2 / 32 -- the same
+                // columns in the same order as the loop below, unrolled, with
+                // the addresses a base and constant strides
+                constexpr int STEP = 32 / PT, NCOL = PT * PT / 32;
+                const int i0 = lane / PT, jl = lane % PT;
+                const T* col0 = tile + (r0 + i0) * PL + (r1 + jl) * Ep + 2 * q0;
+                const int cstep = STEP * PL;
 #pragma unroll
-                for (int q = 0; q < NQC; q++) {
-                    if (PT || q < nq) {
+                for (int m = 0; m < NCOL; m++) {
+                    const T* col = col0 + m * cstep;
+                    VT s0 = PV::zero(), s1 = PV::zero();
+#pragma unroll
+                    for (int q = 0; q < NQC; q++) {
                         const VT g2 = PV::load(col + 2 * q);
                         s0 = PV::fma(g2, wz2[q], s0);
                         if (force) s1 = PV::fma(g2, fz2[q], s1);
                     }
-                }
-                const T t0 = PV::sum(s0);
-                const T wxi = W.wx[i];
-                if (JFIX) {   // j is the lane's own: the y weights multiply once below
+                    const T t0 = PV::sum(s0);
+                    const T wxi = W.wx[i0 + m * STEP];
                     a_pot = fma(t0, wxi, a_pot);
                     if (force) {
-                        a_fx = fma(t0, W.fx[i], a_fx);
+                        a_fx = fma(t0, W.fx[i0 + m * STEP], a_fx);
                         a_fz = fma(PV::sum(s1), wxi, a_fz);
                     }
-                } else {
-                    const T wyj = W.wy[j];
-                    const T wij = wxi * wyj;
-                    a_pot = fma(t0, wij, a_pot);
-                    if (force) {
-                        a_fx = fma(t0, W.fx[i] * wyj, a_fx);
-                        a_fy = fma(t0, wxi * W.fy[j], a_fy);
-                        a_fz = fma(PV::sum(s1), wij, a_fz);
+                }
+            } else {
+                for (int c = lane; c < P * P; c += 32) {
+                    const int i = c / P, j = c - (c / P) * P;
+                    const T* col = tile + (r0 + i) * PL + (r1 + j) * Ep + 2 * q0;
+                    VT s0 = PV::zero(), s1 = PV::zero();
+#pragma unroll
+                    for (int q = 0; q < NQC; q++) {
+                        if (PT || q < nq) {
+                            const VT g2 = PV::load(col + 2 * q);
+                            s0 = PV::fma(g2, wz2[q], s0);
+                            if (force) s1 = PV::fma(g2, fz2[q], s1);
+                        }
+                    }
+                    const T t0 = PV::sum(s0);
+                    const T wxi = W.wx[i];
+                    if (JFIX) {   // j is the lane's own: the y weights multiply once below
+                        a_pot = fma(t0, wxi, a_pot);
+                        if (force) {
+                            a_fx = fma(t0, W.fx[i], a_fx);
+                            a_fz = fma(PV::sum(s1), wxi, a_fz);
+                        }
+                    } else {
+                        const T wyj = W.wy[j];
+                        const T wij = wxi * wyj;
+                        a_pot = fma(t0, wij, a_pot);
+                        if (force) {
+                            a_fx = fma(t0, W.fx[i] * wyj, a_fx);
+                            a_fy = fma(t0, wxi * W.fy[j], a_fy);
+                            a_fz = fma(PV::sum(s1), wij, a_fz);
+                        }
                     }
                 }
             }

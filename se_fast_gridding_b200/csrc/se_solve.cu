@@ -10,7 +10,7 @@
 //   k_factors   each particle's separable Gaussian factors, FGG recurrence
 //   k_spread    one CTA per output tile of the periodic grid, the fold fused
 //               (se_spread.cuh)
-//   cuFFT D2Z, k_scale_rows (Z of scaling(), SE_general.c:145-175, applied to the
+//   cuFFT D2Z, k_scale (Z of scaling(), SE_general.c:145-175, applied to the
 //               half spectrum as product_rc does, SE_general.c:336-362), Z2D
 //   k_interp    one CTA per fine bin, the unfold fused (se_interp.cuh)
 //
@@ -223,74 +223,61 @@ __device__ __forceinline__ double kwave(int i, int M, double kfac)
 
 // spec *= Z on the half spectrum [x][y][z <= M/2]; Z = exp(scalar K2)/K2 * 4pi/M^3
 // with K2 summed in the reference's order (its first FFT axis is our z).
-//
-// One block of SCALE_THREADS takes SCALE_ROWS (x, y) rows of one system.  The
-// grid is cubic, so k^2 and exp(scalar k^2) of the M wave numbers of one axis
-// go into a shared table first, and exp(scalar K2) is the product of three
-// table entries (a few ulps from the exponential of the sum, far inside the
-// FP64 tolerance).  The threads form rows_per_pass groups of TZ = M/2 rounded
-// up to a warp (at most SCALE_THREADS): a group takes z < Mh - 1 of one row
-// (Mh = M/2 + 1) while the other groups take the next rows, and the rows'
-// last z go one per thread at the end.
-constexpr int SCALE_ROWS = 32, SCALE_THREADS = 256;
+constexpr int SCALE_THREADS = 256, SCALE_ITEMS = 8;
 
-
-template <typename V>
-__device__ __forceinline__ void scale_by(V& v, double Z);
-
-template <>
-__device__ __forceinline__ void scale_by<double2>(double2& v, double Z)
+// Elements e = blockIdx.x * SCALE_THREADS * SCALE_ITEMS + ... of the half
+// spectrum [x][y][z <= M/2] of system order[first + blockIdx.y]; 32-bit
+// index arithmetic.
+__global__ void __launch_bounds__(SCALE_THREADS) k_scale(const SysDev* __restrict__ sys,
+                                                         const int* __restrict__ order, int first,
+                                                         double2* __restrict__ spec)
 {
-    v.x *= Z;
-    v.y *= Z;
-}
-
-template <>
-__device__ __forceinline__ void scale_by<float2>(float2& v, double Z)
-{
-    v.x = (float)((double)v.x * Z);
-    v.y = (float)((double)v.y * Z);
-}
-
-// Rows blockIdx.x * SCALE_ROWS + [0, SCALE_ROWS) of system order[first +
-// blockIdx.y] (order NULL: system blockIdx.y); dynamic shared memory of
-// 2 M doubles for the largest M launched.
-template <typename V>
-__global__ void __launch_bounds__(SCALE_THREADS) k_scale_rows(const SysDev* __restrict__ sys,
-                                                              const int* __restrict__ order,
-                                                              int first, V* __restrict__ spec)
-{
-    extern __shared__ double ktab[];   // [0, M): k^2; [M, 2M): exp(scalar k^2)
-    const SysDev& S = sys[order ? order[first + blockIdx.y] : blockIdx.y];
+    const SysDev& S = sys[order[first + blockIdx.y]];
     const int M = S.M, Mh = M / 2 + 1;
-    const int r0 = blockIdx.x * SCALE_ROWS;
-    if (r0 >= M * M) return;   // a smaller grid than the launch's largest
-    for (int i = threadIdx.x; i < M; i += SCALE_THREADS) {
-        const double k = kwave(i, M, S.kfac);
-        const double k2 = k * k;
-        ktab[i] = k2;
-        ktab[M + i] = exp(S.scalar * k2);
-    }
-    __syncthreads();
-    V* sp = spec + S.spec_off;
-    const int nrow = min(SCALE_ROWS, M * M - r0);
-    const int tz = min(SCALE_THREADS, max(32, (M / 2 + 31) / 32 * 32));
-    const int rpp = SCALE_THREADS / tz;   // rows per pass
-    auto one = [&](int r, int iz) {
+    const int n = M * M * Mh;
+    double2* sp = spec + S.spec_off;
+    const int e0 = blockIdx.x * (SCALE_THREADS * SCALE_ITEMS) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < SCALE_ITEMS; k++) {
+        const int e = e0 + k * SCALE_THREADS;
+        if (e >= n) break;
+        const int r = e / Mh, iz = e - r * Mh;
         const int ix = r / M, iy = r - ix * M;
-        const long long e = (long long)r * Mh + iz;
-        const double K2 = (ktab[iz] + ktab[iy]) + ktab[ix];
-        const double Z =
-            (e == 0) ? 0.0 : ktab[M + ix] * ktab[M + iy] * ktab[M + iz] / K2 * S.dnorm;
-        V v = sp[e];
-        scale_by(v, Z);
+        const double kx = kwave(ix, M, S.kfac), ky = kwave(iy, M, S.kfac),
+                     kz = kwave(iz, M, S.kfac);
+        const double K2 = (kz * kz + ky * ky) + kx * kx;
+        const double Z = (e == 0) ? 0.0 : exp(S.scalar * K2) / K2 * S.dnorm;
+        double2 v = sp[e];
+        v.x *= Z;
+        v.y *= Z;
         sp[e] = v;
-    };
-    const int sub = threadIdx.x / tz, z0 = threadIdx.x - sub * tz;
-    if (sub < rpp)
-        for (int rr = sub; rr < nrow; rr += rpp)
-            for (int iz = z0; iz < Mh - 1; iz += tz) one(r0 + rr, iz);
-    for (int rr = threadIdx.x; rr < nrow; rr += SCALE_THREADS) one(r0 + rr, Mh - 1);
+    }
+}
+
+// The same Z, computed in FP64, applied to an FP32 half spectrum.
+__global__ void __launch_bounds__(SCALE_THREADS) k_scale32(const SysDev* __restrict__ sys,
+                                                           float2* __restrict__ spec)
+{
+    const SysDev& S = sys[blockIdx.y];
+    const int M = S.M, Mh = M / 2 + 1;
+    const int n = M * M * Mh;
+    float2* sp = spec + S.spec_off;
+    const int e0 = blockIdx.x * (SCALE_THREADS * SCALE_ITEMS) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < SCALE_ITEMS; k++) {
+        const int e = e0 + k * SCALE_THREADS;
+        if (e >= n) break;
+        const int r = e / Mh, iz = e - r * Mh;
+        const int ix = r / M, iy = r - ix * M;
+        const double kx = kwave(ix, M, S.kfac), ky = kwave(iy, M, S.kfac),
+                     kz = kwave(iz, M, S.kfac);
+        const double K2 = (kz * kz + ky * ky) + kx * kx;
+        const double Z = (e == 0) ? 0.0 : exp(S.scalar * K2) / K2 * S.dnorm;
+        float2 v = sp[e];
+        v.x = (float)((double)v.x * Z);
+        v.y = (float)((double)v.y * Z);
+        sp[e] = v;
+    }
 }
 
 #include "se_fft.cuh"
@@ -1076,10 +1063,9 @@ static int run_kspace32(se_batch b, const double* grid, cudaStream_t st)
     }
     int maxM = 0;
     for (auto& g : b->groups) maxM = std::max(maxM, g.M);
-    const dim3 gs(ceil_div((long)maxM * maxM, SCALE_ROWS), b->nsys);
-    SE_CUDA(raise_smem_limit((const void*)k_scale_rows<float2>, 16 * (size_t)maxM));
-    k_scale_rows<float2><<<gs, SCALE_THREADS, 16 * (size_t)maxM, st>>>(b->sys, nullptr, 0,
-                                                                             b->spec32);
+    const dim3 gs(ceil_div((long)maxM * maxM * (maxM / 2 + 1), SCALE_THREADS * SCALE_ITEMS),
+                  b->nsys);
+    k_scale32<<<gs, SCALE_THREADS, 0, st>>>(b->sys, b->spec32);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
     for (auto& g : b->groups) {
@@ -1131,10 +1117,9 @@ static int run_kspace(se_batch b, double* grid, cudaStream_t st, bool* grid32_fr
         SE_CUFFT(cufftSetStream(g.fwd, st));
         SE_CUFFT(cufftExecD2Z(g.fwd, grid + g.grid_off,
                               reinterpret_cast<cufftDoubleComplex*>(b->spec + g.spec_off)));
-        const dim3 gs(ceil_div((long)g.M * g.M, SCALE_ROWS), g.count);
-        SE_CUDA(raise_smem_limit((const void*)k_scale_rows<double2>, 16 * (size_t)g.M));
-        k_scale_rows<double2><<<gs, SCALE_THREADS, 16 * (size_t)g.M, st>>>(
-            b->sys, b->d_order, g.first, b->spec);
+        const dim3 gs(ceil_div((long)g.M * g.M * (g.M / 2 + 1), SCALE_THREADS * SCALE_ITEMS),
+                      g.count);
+        k_scale<<<gs, SCALE_THREADS, 0, st>>>(b->sys, b->d_order, g.first, b->spec);
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
         SE_CUFFT(cufftSetStream(g.bwd, st));
