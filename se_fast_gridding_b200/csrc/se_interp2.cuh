@@ -320,19 +320,32 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     const T* gs = grid + S.grid_off;
     const int warp = threadIdx.x >> 5;
 
-    // ---- stage the window: rows (a, b), groups of 4 cells along z
+    // ---- stage the window: rows (a, b), groups of 4 cells along z; thread t
+    // copies group t % ng of rows t / ng, t / ng + R, ... (R rows per pass),
+    // stepping (a, b) instead of dividing for every group
     {
         constexpr int G = 4;
         const int ng = EZ / G;
-        for (int u = threadIdx.x; u < E * E * ng; u += blockDim.x) {
-            const int row = u / ng, g = u - row * ng;
-            const int a = row / E, b = row - a * E;
-            int x = o0 + a, y = o1 + b, z = o2 + g * G;
+        const int R = blockDim.x / ng;
+        const int g = threadIdx.x % ng, r0 = threadIdx.x / ng;
+        const int Ra = R / E, Rb = R - Ra * E;
+        int a = r0 / E, b = r0 - a * E;
+        int z = o2 + g * G;
+        z -= z >= M ? M : 0;
+        const T* gz = gs + z;
+        T* tz = tile + g * G;
+        for (int row = r0 < R ? r0 : E * E; row < E * E; row += R) {
+            int x = o0 + a, y = o1 + b;
             x -= x >= M ? M : 0;
             y -= y >= M ? M : 0;
-            z -= z >= M ? M : 0;
-            const T* src = gs + ((long long)x * M + y) * M + z;
-            T* dst = tile + a * PL + b * Ep + g * G;
+            const T* src = gz + ((long long)x * M + y) * M;
+            T* dst = tz + a * PL + b * Ep;
+            a += Ra;
+            b += Rb;
+            if (b >= E) {
+                b -= E;
+                a++;
+            }
 #if SE_I2_ASYNC_STAGE
             // straight into shared memory: two copies of a cell pair each
             // (the window's rows are 8-byte aligned in FP32, 16 in FP64)

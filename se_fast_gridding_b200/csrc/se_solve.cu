@@ -387,6 +387,10 @@ struct se_batch_s {
     unsigned* tp_counter = nullptr;
     double* slab = nullptr;
     int slab_slots = 0;
+    // k_spread2<float>'s CTAs per SM: S2_BLOCKS_FEW when every tile's CTA is
+    // resident at once with 4 per SM (more registers, the same sums), else
+    // S2_BLOCKS_MANY
+    bool spread2_few = false;
     bool any_spread1 = false, any_spread2 = false;   // some system on k_spread / k_spread2
     bool any_interp1 = false, any_interp2 = false;   // on k_interp(_global) / k_interp2
     bool runtime_p = false;                          // some system asks for runtime P
@@ -792,6 +796,12 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     b->ntot = pcur;
     b->nbins = bcur;
     b->ntiles = tcur;
+    {
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+            b->spread2_few = b->ntiles <= S2_BLOCKS_FEW * sms;
+    }
     b->interp_smem = interp_smem_bytes(b->max_P, precision);
     b->plane = interp_plane(b->max_P);
     b->staged_interp = b->interp_smem + sizeof(InterpWarpSmem<double>) * INTERP_WARPS <= 220 * 1024;
@@ -911,7 +921,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         if (r != CUFFT_SUCCESS) return fail(cufft_fail(r, "cufftPlanMany"));
     }
     {
-        // the spread tiles want five CTAs of ~37 KB shared memory per SM
+        // the spread tiles want up to five CTAs of ~43 KB shared memory per SM
         const int carve = (int)cudaSharedmemCarveoutMaxShared;
         cudaError_t a = cudaFuncSetAttribute((const void*)k_spread<float>,
                                              cudaFuncAttributePreferredSharedMemoryCarveout, carve);
@@ -919,10 +929,13 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
             a = cudaFuncSetAttribute((const void*)k_spread<double>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         if (a == cudaSuccess)
-            a = cudaFuncSetAttribute((const void*)k_spread2<float>,
+            a = cudaFuncSetAttribute((const void*)k_spread2<float, S2_BLOCKS_MANY>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         if (a == cudaSuccess)
-            a = cudaFuncSetAttribute((const void*)k_spread2<double>,
+            a = cudaFuncSetAttribute((const void*)k_spread2<float, S2_BLOCKS_FEW>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (a == cudaSuccess)
+            a = cudaFuncSetAttribute((const void*)k_spread2<double, S2_BLOCKS_FP64>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
     }
@@ -1002,12 +1015,13 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
         if (b->precision == SE_FP32)
-            k_spread2<float><<<bound, S2_THREADS, 0, st>>>(
-                b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
-                static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
-                b->tile_done, b->slab, b->slab_slots, b->err);
+            (b->spread2_few ? k_spread2<float, S2_BLOCKS_FEW> : k_spread2<float, S2_BLOCKS_MANY>)
+                <<<bound, S2_THREADS, 0, st>>>(
+                    b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
+                    static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
+                    b->tile_done, b->slab, b->slab_slots, b->err);
         else
-            k_spread2<double><<<bound, S2_THREADS, 0, st>>>(
+            k_spread2<double, S2_BLOCKS_FP64><<<bound, S2_THREADS, 0, st>>>(
                 b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
                 static_cast<const double*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
                 b->tile_done, b->slab, b->slab_slots, b->err);

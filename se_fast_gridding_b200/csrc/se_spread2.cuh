@@ -11,47 +11,60 @@
 // home + h is R[16h .. 16h + 15]: one aligned 64-byte copy, no wrap logic.
 //
 // One CTA of 4 warps owns one 16^3 tile; warp w = 2 wy + wz owns the
-// 16 x 8 x 8 block of y in 8 wy + [0, 8) and z in 8 wz + [0, 8), and after
-// the CTA has listed the bin segments that reach the tile the warps run
-// independently, with no CTA barrier: each warp walks the candidates of the
-// segments in order, keeps the particles whose stencil meets its block, and
-// streams them in groups -- one particle per lane -- through two
-// shared-memory stages that cp.async fills from the factor rows while the
-// warp works on the other: the x tile row, the warp's 8 y and 8 z entries and
-// the charge.  Each lane adds px[x] * (q py[y] pz[z]) into 16 x 2 cells (all
-// 16 x of its (y, z) and (y, z + 1)).  Every cell belongs to one lane of one CTA: no atomics and a
-// fixed order of summation (the particles' candidate order).  FP32:
-// packed FP32 pair FMAs on the cells, and after every 512 of the warp's
-// particles the FP32 sums are added into the FP64 grid in place (the first
-// time stored), which the lane alone reads and writes.
+// 16 x 8 x 8 block of y in 8 wy + [0, 8) and z in 8 wz + [0, 8), and the
+// warps run independently, with no CTA barrier.  A warp lists the bin
+// segments whose particles may reach its block (the tile's 16 x cells, its
+// own 8 y and 8 z: at most 5 x 4 x 2 segments), walks their candidates in
+// order, keeps the particles whose stencil meets the block and sorts them
+// into three x classes -- the particle's x row in the tile meets both 8-cell
+// halves, the low half only or the high half only -- one list ring each.
+// Whenever a class holds a group (one particle per lane) the warp streams it
+// through two shared-memory stages that cp.async fills from the factor rows
+// while the warp works on the other: the x tile row (of a one-half class,
+// that half), the warp's 8 y and 8 z entries and the charge.  Each lane adds
+// px[x] * (q py[y] pz[z]) into the 16 x 2 cells of its (y, z) and
+// (y, z + 1), or the 8 x 2 of the class's half: a one-half group costs half
+// the FMAs of a full one, and a particle is a one-half particle in about
+// half of the tiles it meets at P = 16 (more at smaller P).  Every cell
+// belongs to one lane of one CTA: no atomics and a fixed order of summation
+// (the groups' order, which depends only on the block's candidate list).
+// FP32: packed FP32 pair FMAs on the cells, and after every 512 of the
+// warp's particles the FP32 sums are added into the FP64 grid in place (the
+// first time stored), which the lane alone reads and writes.
 //
-// Crowded tiles are split.  A tile's candidate list (the particles of the
-// bin segments that reach it, in bin order) is cut into parts of at most
-// S2_CAP candidates; k_tile_parts counts each tile's candidates and scans the
-// part counts, and k_spread2 runs one CTA per part.  Part 0 writes the tile
-// into the grid as above; part s >= 1 writes its sums into slab slot
-// (extra parts of the tiles before it) + s - 1, 16^3 FP64 cells; the part
-// that finishes last (a per-tile counter) adds the slabs into the grid in
-// the order s = 1, 2, ...  A tile's parts and their sums depend only on its
-// own candidates, so results stay deterministic and a batched system's grid
-// equals its single solve's.  Uniform inputs at the configurations' densities
-// have far fewer than S2_CAP candidates per tile and are never split.
+// Crowded tiles are split.  Each warp's candidate list is cut into parts of
+// at most S2_CAP candidates; k_tile_parts counts the candidates of each
+// tile's most crowded block and scans the part counts, and k_spread2 runs
+// one CTA per part, whose warps take part s of their own lists.  Part 0
+// writes the tile into the grid as above; part s >= 1 writes its sums into
+// slab slot (extra parts of the tiles before it) + s - 1, 16^3 FP64 cells;
+// the part that finishes last (a per-tile counter) adds the slabs into the
+// grid in the order s = 1, 2, ...  A tile's parts and their sums depend only
+// on its own candidates, so results stay deterministic and a batched
+// system's grid equals its single solve's.  Uniform inputs at the
+// configurations' densities have far fewer than S2_CAP candidates per block
+// and are never split.
 
 #ifndef SE_S2_CAP
 #define SE_S2_CAP 8192
 #endif
-#ifndef SE_S2_MIN_BLOCKS
-#define SE_S2_MIN_BLOCKS 5
+#ifndef SE_S2_UNROLL
+#define SE_S2_UNROLL 16
 #endif
-#ifndef SE_S2_FULL_GROUP
-#define SE_S2_FULL_GROUP 1
-#endif
-constexpr int S2_CAP = SE_S2_CAP;   // candidates per part of a tile
+constexpr int S2_CAP = SE_S2_CAP;   // candidates per part of a warp's list
 constexpr int S2_WARPS = 4;
 constexpr int S2_THREADS = S2_WARPS * 32;
-constexpr int S2_LIST = 64;    // per-warp list ring: >= group - 1 + 32
-constexpr int S2_SEGS = 64;    // bin segments reaching a tile: <= 5 x 5 x 2 for P <= 16
+constexpr int S2_LIST = 64;    // per-class list ring: >= group - 1 + 32
+constexpr int S2_SEGS = 64;    // bin segments reaching a warp's block: <= 5 x 4 x 2 for P <= 16
 constexpr int S2_FOLD = 512;   // FP32 partial sums cover this many of a warp's particles
+// x classes of a particle in a tile: its x row meets both 8-cell halves,
+// the low half only, the high half only
+constexpr int S2_CLASSES = 3;
+constexpr int S2_UNROLL = SE_S2_UNROLL;   // particles per unrolled pass of a group
+// FP32 CTAs per SM the kernel is compiled for: 5 (96 registers) where the
+// tiles outnumber 4 CTAs per SM, 4 (128 registers) where all of them are
+// resident at once either way; FP64: 3
+constexpr int S2_BLOCKS_MANY = 5, S2_BLOCKS_FEW = 4, S2_BLOCKS_FP64 = 3;
 
 // particles a warp stages at once: one per lane (FP32), half a warp (FP64)
 template <typename Acc>
@@ -68,10 +81,9 @@ struct Spread2Stage {
 template <typename Acc>
 struct Spread2Smem {
     Spread2Stage<Acc> stage[S2_WARPS][2];
-    int2 list[S2_WARPS][S2_LIST];   // (particle, packed grid index)
-    int seg_beg[S2_SEGS];
-    int seg_pre[S2_SEGS];
-    int wsum[S2_WARPS];
+    int2 list[S2_WARPS][S2_CLASSES][S2_LIST];   // (particle, packed grid index)
+    int seg_beg[S2_WARPS][S2_SEGS];
+    int seg_pre[S2_WARPS][S2_SEGS];
 };
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc)
@@ -109,6 +121,22 @@ struct Spread2Accum<float> {
         const float4* p4 = reinterpret_cast<const float4*>(px);
 #pragma unroll
         for (int m = 0; m < 4; m++) {
+            float2 lo, hi;
+            f32x2_split(p4[m], lo, hi);
+            a[2 * m] = ffma2(lo, k0, a[2 * m]);
+            a[2 * m + 1] = ffma2(hi, k0, a[2 * m + 1]);
+            b[2 * m] = ffma2(lo, k1, b[2 * m]);
+            b[2 * m + 1] = ffma2(hi, k1, b[2 * m + 1]);
+        }
+    }
+    // x in [8 H, 8 H + 8) only (the row is zero on the other half)
+    template <int H>
+    __device__ __forceinline__ void add_half(const float* px, float c0, float c1)
+    {
+        const float2 k0 = f32x2(c0, c0), k1 = f32x2(c1, c1);
+        const float4* p4 = reinterpret_cast<const float4*>(px);
+#pragma unroll
+        for (int m = 2 * H; m < 2 * H + 2; m++) {
             float2 lo, hi;
             f32x2_split(p4[m], lo, hi);
             a[2 * m] = ffma2(lo, k0, a[2 * m]);
@@ -162,6 +190,19 @@ struct Spread2Accum<double> {
             b[2 * m + 1] = fma(w.y, c1, b[2 * m + 1]);
         }
     }
+    template <int H>
+    __device__ __forceinline__ void add_half(const double* px, double c0, double c1)
+    {
+        const double2* p2 = reinterpret_cast<const double2*>(px);
+#pragma unroll
+        for (int m = 4 * H; m < 4 * H + 4; m++) {
+            const double2 w = p2[m];
+            a[2 * m] = fma(w.x, c0, a[2 * m]);
+            a[2 * m + 1] = fma(w.y, c0, a[2 * m + 1]);
+            b[2 * m] = fma(w.x, c1, b[2 * m]);
+            b[2 * m + 1] = fma(w.y, c1, b[2 * m + 1]);
+        }
+    }
     __device__ __forceinline__ void store(double* cell0, long long plane) const
     {
 #pragma unroll
@@ -180,33 +221,64 @@ __device__ __forceinline__ int tile_half(int g, int ti, int nt, int P)
     return (h == 1 && (g & 15) + P > 16) ? 1 : -1;
 }
 
-// The number of candidates of tile lt of system S (the particles of the bin
-// segments that reach it), summed over the warp; every lane gets it.
+// The bins whose particles may reach block (wy, wz) of a tile at corner
+// (x0, y0, z0) -- x: the tile's 16 cells, y and z: the block's 8 -- as
+// segments (x bin, y bin, z run) numbered x-major; a z run is a contiguous
+// range of bins, so a segment is a contiguous range of the sorted particles.
+struct BlockBins {
+    BinRanges rx, ry, rz;
+    int nx, ny;
+    __device__ __forceinline__ BlockBins(const SysDev& S, int x0, int y0, int z0)
+        : rx(bins_reaching(x0, 16, S.M, S.P, S.nf[0])),
+          ry(bins_reaching(y0, 8, S.M, S.P, S.nf[1])),
+          rz(bins_reaching(z0, 8, S.M, S.P, S.nf[2])),
+          nx(range_count(rx)), ny(range_count(ry))
+    {
+    }
+    __device__ __forceinline__ int segments() const { return nx * ny * 2; }
+    // the particles [beg, beg + len) of segment u
+    __device__ __forceinline__ void segment(const SysDev& S, const int* __restrict__ boff, int u,
+                                            int& beg, int& len) const
+    {
+        const int zr = u & 1, iy = (u >> 1) % ny, ix = (u >> 1) / ny;
+        const int bz0 = zr ? rz.b0 : rz.a0, bz1 = zr ? rz.b1 : rz.a1;
+        beg = 0;
+        len = 0;
+        if (bz0 <= bz1) {
+            const int kb = S.bin_base + (range_at(rx, ix) * S.nf[1] + range_at(ry, iy)) * S.nf[2];
+            beg = boff[kb + bz0];
+            len = boff[kb + bz1 + 1] - beg;
+        }
+    }
+};
+
+// The largest number of candidates (the particles of the bin segments that
+// reach a block) over the four warp blocks of tile lt of system S; every
+// lane gets it.
 __device__ __forceinline__ int tile_candidates(const SysDev& S, int lt, const int* __restrict__ boff,
                                                int lane)
 {
     const int nt = S.nt[0];
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
-    const BinRanges rx = bins_reaching(tix * 16, 16, S.M, S.P, S.nf[0]);
-    const BinRanges ry = bins_reaching(tiy * 16, 16, S.M, S.P, S.nf[1]);
-    const BinRanges rz = bins_reaching(tiz * 16, 16, S.M, S.P, S.nf[2]);
-    const int nx = range_count(rx), ny = range_count(ry);
-    int sum = 0;
-    for (int u = lane; u < nx * ny * 2; u += 32) {
-        const int zr = u & 1, iy = (u >> 1) % ny, ix = (u >> 1) / ny;
-        const int bz0 = zr ? rz.b0 : rz.a0, bz1 = zr ? rz.b1 : rz.a1;
-        if (bz0 <= bz1) {
-            const int kb = S.bin_base + (range_at(rx, ix) * S.nf[1] + range_at(ry, iy)) * S.nf[2];
-            sum += boff[kb + bz1 + 1] - boff[kb + bz0];
+    int most = 0;
+    for (int w = 0; w < S2_WARPS; w++) {
+        const BlockBins B(S, tix * 16, tiy * 16 + 8 * (w >> 1), tiz * 16 + 8 * (w & 1));
+        int sum = 0;
+        for (int u = lane; u < B.segments(); u += 32) {
+            int beg, len;
+            B.segment(S, boff, u, beg, len);
+            sum += len;
         }
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    return sum;
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        most = max(most, sum);
+    }
+    return most;
 }
 
 // Parts per tile (one warp per tile: max(1, ceil(candidates / S2_CAP)) for
-// the k_spread2 systems, 1 for the others), then, in the block that finishes
+// the k_spread2 systems, candidates of its most crowded block; 1 for the
+// others), then, in the block that finishes
 // last, their exclusive scan in place: parts[t] = the first part of tile t,
 // parts[ntiles] = the number of parts.  More parts than the launch bound
 // (which no input reaches: a bin is a candidate of at most two tiles per
@@ -276,8 +348,8 @@ __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
     }
 }
 
-template <typename Acc>
-__global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCKS : 3) k_spread2(
+template <typename Acc, int BLOCKS>
+__global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid,
@@ -320,46 +392,37 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
     const int ly = lane >> 2, lz = (lane & 3) * 2;
     const unsigned ybits = 0xFFu << (8 * wy), zbits = 0xFFu << (8 * wz);
 
-    // ---- the bin segments reaching this tile (at most 5 x 5 x 2) and their prefix
-    const BinRanges rx = bins_reaching(x0, 16, M, P, S.nf[0]);
-    const BinRanges ry = bins_reaching(y0, 16, M, P, S.nf[1]);
-    const BinRanges rz = bins_reaching(z0, 16, M, P, S.nf[2]);
-    const int nx = range_count(rx), ny = range_count(ry);
-    const int nseg = nx * ny * 2;
-    int beg = 0, len = 0;
-    if (t < nseg) {
-        const int zr = t & 1, iy = (t >> 1) % ny, ix = (t >> 1) / ny;
-        const int bz0 = zr ? rz.b0 : rz.a0, bz1 = zr ? rz.b1 : rz.a1;
-        if (bz0 <= bz1) {
-            const int kb = S.bin_base + (range_at(rx, ix) * S.nf[1] + range_at(ry, iy)) * S.nf[2];
-            beg = boff[kb + bz0];
-            len = boff[kb + bz1 + 1] - beg;
+    // ---- the bin segments reaching this warp's block (at most 5 x 4 x 2) and
+    // their prefix: the warp's own candidate list, in segment order
+    const BlockBins B(S, x0, y0 + 8 * wy, z0 + 8 * wz);
+    int nseg = B.segments();
+    if (nseg > S2_SEGS) {   // cannot happen for M >= 32 and P <= 16: flagged, the block sums nothing
+        if (lane == 0) atomicOr(err, 2);
+        nseg = 0;
+    }
+    int* seg_beg = sm.seg_beg[warp];
+    int* seg_pre = sm.seg_pre[warp];
+    int total = 0;
+    for (int u0 = 0; u0 < nseg; u0 += 32) {
+        const int u = u0 + lane;
+        int beg = 0, len = 0;
+        if (u < nseg) B.segment(S, boff, u, beg, len);
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
         }
+        if (u < nseg) {
+            seg_beg[u] = beg;
+            seg_pre[u] = total + incl - len;
+        }
+        total += __shfl_sync(0xffffffffu, incl, 31);
     }
-    int incl = len;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) sm.wsum[warp] = incl;
-    __syncthreads();
-    int before = 0, total = 0;
-#pragma unroll
-    for (int w = 0; w < S2_WARPS; w++) {
-        const int v = sm.wsum[w];
-        before += w < warp ? v : 0;
-        total += v;
-    }
-    if (t < S2_SEGS) {
-        sm.seg_beg[t] = beg;
-        sm.seg_pre[t] = before + incl - len;
-    }
-    __syncthreads();   // the last CTA barrier: from here on the warps are independent
+    __syncwarp();   // the warps are independent from here on
 
     const unsigned pmask = (1u << P) - 1u;   // P <= 16
     const unsigned lanes_before = (1u << lane) - 1u;
-    int2* list = sm.list[warp];
     double* gs = grid + S.grid_off;
     const long long gplane = (long long)M * M;
     // part 0 sums into the grid, the others into their slab slot
@@ -368,43 +431,65 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
     double* cell0 =
         ipart == 0 ? gs + (long long)x0 * gplane + (long long)(y0 + 8 * wy + ly) * M + z0 + 8 * wz + lz
                   : slab + (long long)(slot0 + ipart - 1) * 4096 + (8 * wy + ly) * 16 + 8 * wz + lz;
-    // this part's candidates: [cbeg, cend) of the tile's list
+    // this part's candidates: [cbeg, cend) of the warp's list
     const int cbeg = ipart * S2_CAP, cend = min(total, cbeg + S2_CAP);
 
     Spread2Accum<Acc> acc;
     acc.zero();
-    int cpos = cbeg, head = 0, tail = 0, buf = 0, pending = 0, since_fold = 0;
+    // one ring per x class: byte c of cnt holds the entries of class c
+    // listed and not yet staged (< 64), byte c of ring the slot of the first
+    unsigned cnt = 0u, ring = 0u;
+    // a class holds a group when its count has a bit of value >= G
+    constexpr unsigned FULL = (G == 32 ? 0x20u : 0x30u) * 0x010101u;
+    int cpos = cbeg, buf = 0, pending = 0, pcls = 0, since_fold = 0;
     int seg = 0;   // the segment holding candidate cpos
-    while (seg + 1 < nseg && sm.seg_pre[seg + 1] <= cpos) seg++;
+    while (seg + 1 < nseg && seg_pre[seg + 1] <= cpos) seg++;
     bool written = false;
     for (;;) {
-        // ---- list at least a group (or every remaining candidate), in order
-        while (tail - head < G && cpos < cend) {
+        // ---- list until some class holds a group (or every remaining
+        // candidate is listed), each class in candidate order
+        while (!(cnt & FULL) && cpos < cend) {
             const int pos = cpos + lane;
-            int part = -1, pk = 0, sl = seg;   // this lane's segment, found forward
+            int part = -1, pk = 0, cls = -1, sl = seg;   // this lane's segment, found forward
             if (pos < cend) {
-                while (sl + 1 < nseg && sm.seg_pre[sl + 1] <= pos) sl++;
-                part = sm.seg_beg[sl] + (pos - sm.seg_pre[sl]);
+                while (sl + 1 < nseg && seg_pre[sl + 1] <= pos) sl++;
+                part = seg_beg[sl] + (pos - seg_pre[sl]);
                 pk = sg[part];
                 // the stencil's cells in this tile, as 16-bit masks per axis
-                const int gy = g_of(pk, 1), gz = g_of(pk, 2);
+                const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
+                const int hx = tile_half(gx, tix, nt, P);
                 const int hy = tile_half(gy, tiy, nt, P), hz = tile_half(gz, tiz, nt, P);
-                const bool meets = tile_half(g_of(pk, 0), tix, nt, P) >= 0 && hy >= 0 &&
-                                   hz >= 0 &&
+                const unsigned xm = ((pmask << (gx & 15)) >> (16 * max(hx, 0))) & 0xFFFFu;
+                const bool meets = hx >= 0 && hy >= 0 && hz >= 0 &&
                                    ((((pmask << (gy & 15)) >> (16 * hy)) & 0xFFFFu) & ybits) &&
                                    ((((pmask << (gz & 15)) >> (16 * hz)) & 0xFFFFu) & zbits);
-                if (!meets) part = -1;
+                if (meets) cls = (xm & 0xFFu) ? ((xm & 0xFF00u) ? 0 : 1) : 2;
             }
-            const unsigned keep = __ballot_sync(0xffffffffu, part >= 0);
-            if (part >= 0)
-                list[(tail + __popc(keep & lanes_before)) & (S2_LIST - 1)] = make_int2(part, pk);
-            tail += __popc(keep);
+            const unsigned k0 = __ballot_sync(0xffffffffu, cls == 0);
+            const unsigned k1 = __ballot_sync(0xffffffffu, cls == 1);
+            const unsigned k2 = __ballot_sync(0xffffffffu, cls == 2);
+            if (cls >= 0) {
+                const unsigned kc = cls == 0 ? k0 : (cls == 1 ? k1 : k2);
+                const int sh = 8 * cls;
+                sm.list[warp][cls][((ring >> sh) + (cnt >> sh) + __popc(kc & lanes_before)) &
+                                   (S2_LIST - 1)] = make_int2(part, pk);
+            }
+            cnt += __popc(k0) | (__popc(k1) << 8) | (__popc(k2) << 16);
             cpos += 32;
             seg = __reduce_max_sync(0xffffffffu, sl);
         }
         __syncwarp();   // list entries visible to the warp
-        // ---- stage the next group: lane l < n copies particle head + l
-        const int n = min(G, tail - head);
+        // ---- the class to stage: a full group if some class has one (the
+        // first such class), else the first class with entries left
+        const unsigned pick = (cnt & FULL) ? (cnt & FULL) : cnt;
+        const int cls = pick ? (__ffs(pick) - 1) >> 3 : 0;
+        const int sh = 8 * cls;
+        const int avail = (cnt >> sh) & 0xFF;
+        const int head = (ring >> sh) & (S2_LIST - 1);
+        const int2* list = sm.list[warp][cls];
+        // ---- stage the next group of the class: lane l < n copies its
+        // particle head + l (of a one-half class, that half of the x row)
+        const int n = min(G, avail);
         if (n > 0) {
             Spread2Stage<Acc>& st = sm.stage[warp][buf];
             if (lane < n) {
@@ -413,27 +498,31 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
                 const int hy = tile_half(g_of(e.y, 1), tiy, nt, P);
                 const int hz = tile_half(g_of(e.y, 2), tiz, nt, P);
                 const Acc* r = rows + (long long)e.x * 96;
+                if (cls == 0) {
 #pragma unroll
-                for (int k = 0; k < 16; k += V) cp_async16(&st.px[lane][k], r + 16 * hx + k);
+                    for (int k = 0; k < 16; k += V) cp_async16(&st.px[lane][k], r + 16 * hx + k);
+                } else {
+                    const int o = 8 * (cls - 1);
+#pragma unroll
+                    for (int k = 0; k < 8; k += V) cp_async16(&st.px[lane][o + k], r + 16 * hx + o + k);
+                }
 #pragma unroll
                 for (int k = 0; k < 8; k += V) {
                     cp_async16(&st.py[lane][k], r + 32 + 16 * hy + 8 * wy + k);
                     cp_async16(&st.pz[lane][k], r + 64 + 16 * hz + 8 * wz + k);
                 }
                 cp_async8(&st.q[lane], &srec[e.x].w);
-            }
-#if SE_S2_FULL_GROUP
-            else if (lane < G) {   // a short (the last) group: zero rows up to G (FP64: 16),
-                                   // so every group sums G rows
+            } else if (lane < G) {   // a short group: zero rows up to G (FP64: 16),
+                                     // so every group sums G rows
 #pragma unroll
                 for (int k = 0; k < 16; k++) st.px[lane][k] = Acc(0);
 #pragma unroll
                 for (int k = 0; k < 8; k++) st.py[lane][k] = st.pz[lane][k] = Acc(0);
                 st.q[lane] = 0.0;
             }
-#endif
             cp_async_commit();
-            head += n;
+            cnt -= (unsigned)n << sh;
+            ring = (ring & ~(0xFFu << sh)) | ((unsigned)((head + n) & (S2_LIST - 1)) << sh);
         }
         __syncwarp();   // the staged entries are read before the list refills over them
         // ---- the previous group, while this one lands
@@ -449,17 +538,27 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
                 for (int k = 0; k < 8; k++) st.py[lane][k] = st.py[lane][k] * qv;
             }
             __syncwarp();
-#if SE_S2_FULL_GROUP
             // every group holds G rows (a short one padded with zeros, which
-            // add exact zeros): one unrolled pass with constant offsets
-#pragma unroll
-            for (int i = 0; i < G; i++) {
-#else
-#pragma unroll 2
-            for (int i = 0; i < pending; i++) {
-#endif
-                const Acc y = st.py[i][ly];
-                acc.add(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
+            // add exact zeros): one unrolled pass per class with constant
+            // offsets; a one-half class touches the lane's 8 x 2 cells of its half
+            if (pcls == 0) {
+#pragma unroll S2_UNROLL
+                for (int i = 0; i < G; i++) {
+                    const Acc y = st.py[i][ly];
+                    acc.add(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
+                }
+            } else if (pcls == 1) {
+#pragma unroll S2_UNROLL
+                for (int i = 0; i < G; i++) {
+                    const Acc y = st.py[i][ly];
+                    acc.template add_half<0>(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
+                }
+            } else {
+#pragma unroll S2_UNROLL
+                for (int i = 0; i < G; i++) {
+                    const Acc y = st.py[i][ly];
+                    acc.template add_half<1>(st.px[i], y * st.pz[i][lz], y * st.pz[i][lz + 1]);
+                }
             }
             if constexpr (FOLD) {
                 since_fold += pending;
@@ -473,6 +572,7 @@ __global__ void __launch_bounds__(S2_THREADS, sizeof(Acc) == 4 ? SE_S2_MIN_BLOCK
         }
         if (n == 0) break;
         pending = n;
+        pcls = cls;
         buf ^= 1;
     }
 
