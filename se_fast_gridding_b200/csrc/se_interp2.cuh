@@ -411,20 +411,25 @@ __device__ __forceinline__ void interp2_columns(
     constexpr int NQ = PT ? PT / 2 + 1 : 9;   // z pairs a stencil spans (<= 9 for P <= 16)
     const int nq = P / 2 + 1;
     for (int p = pfirst; p < pend; p += I2_WARPS) {
+        // the particle's three tile-aligned rows, entry l in lane l, loaded
+        // beside its record: their addresses do not wait for the corner
+        const T* rb = rows + (long long)p * 96;
+        const T ex = rb[lane], ey = rb[32 + lane], ez = rb[64 + lane];
         const double4 rc = srec[p];
         const int pk = sg[p];
         const int orig = sperm[p];
         const int gx = g_of(pk, 0), gy = g_of(pk, 1), gz = g_of(pk, 2);
         const int r0 = gx - o0, r1 = gy - o1, r2 = gz - o2;
-        // weights: lane i < P holds factor i of each axis (tile-aligned rows)
-        const T* rb = rows + (long long)p * 96;
+        // weights: lane i < P holds factor i of each axis, row entry
+        // (g mod 16) + i (<= 30), from the lane that loaded it
+        const T vx = __shfl_sync(0xffffffffu, ex, ((gx & 15) + lane) & 31);
+        const T vy = __shfl_sync(0xffffffffu, ey, ((gy & 15) + lane) & 31);
+        const T vz = __shfl_sync(0xffffffffu, ez, ((gz & 15) + lane) & 31);
         W.wz[lane] = T(0);
         W.fz[lane] = T(0);
         __syncwarp();
         if (lane < P) {
             const double off = (S.lo + lane) * S.h;
-            const T vx = rb[(gx & 15) + lane], vy = rb[32 + (gy & 15) + lane],
-                    vz = rb[64 + (gz & 15) + lane];
             W.wx[lane] = vx;
             W.wy[lane] = vy;
             W.wz[r2 + lane] = vz;

@@ -1009,7 +1009,7 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
         // the parts of each tile, then one CTA per part (at most the bound;
         // the CTAs past the number of parts return at once)
         const int bound = b->ntiles + b->slab_slots;
-        k_tile_parts<<<ceil_div(b->ntiles, TP_WARPS), TP_WARPS * 32, 0, st>>>(
+        k_tile_parts<<<ceil_div(b->ntiles, TP_TILES), TP_WARPS * 32, 0, st>>>(
             b->sys, b->d_tile_prefix, b->nsys, b->ntiles, b->boff, b->tile_parts, b->tp_counter,
             bound, b->err);
         SE_CUDA(cudaGetLastError());

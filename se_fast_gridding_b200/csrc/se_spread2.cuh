@@ -252,54 +252,55 @@ struct BlockBins {
     }
 };
 
-// The largest number of candidates (the particles of the bin segments that
-// reach a block) over the four warp blocks of tile lt of system S; every
-// lane gets it.
-__device__ __forceinline__ int tile_candidates(const SysDev& S, int lt, const int* __restrict__ boff,
-                                               int lane)
+// The number of candidates (the particles of the bin segments that reach
+// it) of warp block w of tile lt of system S; every lane gets it.
+__device__ __forceinline__ int block_candidates(const SysDev& S, int lt, int w,
+                                                const int* __restrict__ boff, int lane)
 {
     const int nt = S.nt[0];
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
-    int most = 0;
-    for (int w = 0; w < S2_WARPS; w++) {
-        const BlockBins B(S, tix * 16, tiy * 16 + 8 * (w >> 1), tiz * 16 + 8 * (w & 1));
-        int sum = 0;
-        for (int u = lane; u < B.segments(); u += 32) {
-            int beg, len;
-            B.segment(S, boff, u, beg, len);
-            sum += len;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        most = max(most, sum);
+    const BlockBins B(S, tix * 16, tiy * 16 + 8 * (w >> 1), tiz * 16 + 8 * (w & 1));
+    int sum = 0;
+    for (int u = lane; u < B.segments(); u += 32) {
+        int beg, len;
+        B.segment(S, boff, u, beg, len);
+        sum += len;
     }
-    return most;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    return sum;
 }
 
-// Parts per tile (one warp per tile: max(1, ceil(candidates / S2_CAP)) for
-// the k_spread2 systems, candidates of its most crowded block; 1 for the
-// others), then, in the block that finishes
+// Parts per tile (one warp per warp block, two tiles per CTA:
+// max(1, ceil(candidates of the most crowded block / S2_CAP)) for the
+// k_spread2 systems, 1 for the others), then, in the block that finishes
 // last, their exclusive scan in place: parts[t] = the first part of tile t,
 // parts[ntiles] = the number of parts.  More parts than the launch bound
 // (which no input reaches: a bin is a candidate of at most two tiles per
 // axis) set bit 2 of err.  The block counter is left at zero for the next
 // launch.
 constexpr int TP_WARPS = 8;
+constexpr int TP_TILES = TP_WARPS / S2_WARPS;   // tiles per CTA
 
 __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys, int ntiles,
     const int* __restrict__ boff, int* parts, unsigned* counter, int bound, int* err)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile = blockIdx.x * TP_WARPS + warp;
+    const int tile = blockIdx.x * TP_TILES + warp / S2_WARPS, wb = warp % S2_WARPS;
+    __shared__ int cand[TP_WARPS];
+    int c = 0;
     if (tile < ntiles) {
         const SysDev& S = sys[find_sys(tile_prefix, nsys, tile)];
-        int n = 1;
-        if (S.path & PATH_TILE_SPREAD) {
-            const int c = tile_candidates(S, tile - S.tile_base, boff, lane);
-            n = max(1, (c + S2_CAP - 1) / S2_CAP);
-        }
-        if (lane == 0) parts[tile] = n;
+        if (S.path & PATH_TILE_SPREAD) c = block_candidates(S, tile - S.tile_base, wb, boff, lane);
+    }
+    if (lane == 0) cand[warp] = c;
+    __syncthreads();
+    if (wb == 0 && lane == 0 && tile < ntiles) {
+        int most = 0;
+#pragma unroll
+        for (int k = 0; k < S2_WARPS; k++) most = max(most, cand[warp + k]);
+        parts[tile] = max(1, (most + S2_CAP - 1) / S2_CAP);
     }
     __shared__ int last;
     __shared__ int wsum[TP_WARPS];
