@@ -449,6 +449,16 @@ def c4_record(args, dev, rank=0):
     del xd, qd, outs
     head = runs[0]
     cap0 = capacity[0]
+    offered = cap0["particles_per_s"] * cap0["wall_s"] / args.serve_seconds
+    limit = {
+        "offered_particles_per_s": offered,
+        "capacity_particles_per_s": cap0["particles_per_s"],
+        "note": "the M-from-N trace offers this many particles/s of spread and interpolation "
+                "(its requests with N > 128k on M=256 grids); the capacity, the whole trace "
+                "submitted at once, is below it, so kernel throughput and not admission bounds "
+                "the served rate" if offered > cap0["particles_per_s"] else
+                "the capacity exceeds the offered particle rate",
+    }
     return {
         "workload": f"serving: Poisson {head['offered_req_s']:.0f} req/s for {args.serve_seconds} s, "
                     "POTENTIAL/FORCE 50/50, N log-uniform [500, 2e6], P in {8,12,16}, L=1, "
@@ -457,6 +467,7 @@ def c4_record(args, dev, rank=0):
         "latency_clock": "host steady clock, submit to result in host memory",
         "solves_per_s": head["solves_per_s"], "p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"],
         "particles_per_s": head["particles_per_s"], "runs": runs, "capacity": capacity,
+        "limit": limit,
         "fp64_plain": {"requests": len(trace), "particles_per_s": parts64 / t64,
                        "solves_per_s": len(trace) / t64,
                        "served_capacity_speedup": cap0["particles_per_s"] / (parts64 / t64),
