@@ -550,12 +550,22 @@ __device__ __forceinline__ void interp2_columns(
 
 // Every FP64 grid value of the batch as FP32 (the staged source of
 // k_interp2<float>), two values per thread step.
+// A thread converts CONVERT_ITEMS pairs a pass, loading them all first; the
+// grid is at most CONVERT_CTAS CTAs of 256 (8 per SM of a B200).
+constexpr int CONVERT_ITEMS = 4, CONVERT_CTAS = 148 * 8;
+
 __global__ void k_grid_to_f32(const double2* __restrict__ in, float2* __restrict__ out,
                               long long n2)
 {
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n2;
-         e += (long long)gridDim.x * blockDim.x) {
-        const double2 v = in[e];
-        out[e] = make_float2((float)v.x, (float)v.y);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < n2;
+         e0 += stride * CONVERT_ITEMS) {
+        double2 v[CONVERT_ITEMS];
+#pragma unroll
+        for (int k = 0; k < CONVERT_ITEMS; k++)
+            if (e0 + k * stride < n2) v[k] = in[e0 + k * stride];
+#pragma unroll
+        for (int k = 0; k < CONVERT_ITEMS; k++)
+            if (e0 + k * stride < n2) out[e0 + k * stride] = make_float2((float)v[k].x, (float)v[k].y);
     }
 }

@@ -237,6 +237,13 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale(const SysDev* __restric
     const int n = M * M * Mh;
     double2* sp = spec + S.spec_off;
     const int e0 = blockIdx.x * (SCALE_THREADS * SCALE_ITEMS) + threadIdx.x;
+    // every load of the thread first, so they are in flight together
+    double2 v[SCALE_ITEMS];
+#pragma unroll
+    for (int k = 0; k < SCALE_ITEMS; k++) {
+        const int e = e0 + k * SCALE_THREADS;
+        if (e < n) v[k] = sp[e];
+    }
 #pragma unroll
     for (int k = 0; k < SCALE_ITEMS; k++) {
         const int e = e0 + k * SCALE_THREADS;
@@ -247,10 +254,9 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale(const SysDev* __restric
                      kz = kwave(iz, M, S.kfac);
         const double K2 = (kz * kz + ky * ky) + kx * kx;
         const double Z = (e == 0) ? 0.0 : exp(S.scalar * K2) / K2 * S.dnorm;
-        double2 v = sp[e];
-        v.x *= Z;
-        v.y *= Z;
-        sp[e] = v;
+        v[k].x *= Z;
+        v[k].y *= Z;
+        sp[e] = v[k];
     }
 }
 
@@ -263,6 +269,12 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale32(const SysDev* __restr
     const int n = M * M * Mh;
     float2* sp = spec + S.spec_off;
     const int e0 = blockIdx.x * (SCALE_THREADS * SCALE_ITEMS) + threadIdx.x;
+    float2 v[SCALE_ITEMS];   // every load first, as in k_scale
+#pragma unroll
+    for (int k = 0; k < SCALE_ITEMS; k++) {
+        const int e = e0 + k * SCALE_THREADS;
+        if (e < n) v[k] = sp[e];
+    }
 #pragma unroll
     for (int k = 0; k < SCALE_ITEMS; k++) {
         const int e = e0 + k * SCALE_THREADS;
@@ -273,10 +285,9 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale32(const SysDev* __restr
                      kz = kwave(iz, M, S.kfac);
         const double K2 = (kz * kz + ky * ky) + kx * kx;
         const double Z = (e == 0) ? 0.0 : exp(S.scalar * K2) / K2 * S.dnorm;
-        float2 v = sp[e];
-        v.x = (float)((double)v.x * Z);
-        v.y = (float)((double)v.y * Z);
-        sp[e] = v;
+        v[k].x = (float)((double)v[k].x * Z);
+        v[k].y = (float)((double)v[k].y * Z);
+        sp[e] = v[k];
     }
 }
 
@@ -289,10 +300,16 @@ __global__ void __launch_bounds__(SCALE_THREADS) k_scale32(const SysDev* __restr
 __global__ void k_grid_to_f64(const float2* __restrict__ in, double2* __restrict__ out,
                               long long n2)
 {
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n2;
-         e += (long long)gridDim.x * blockDim.x) {
-        const float2 v = in[e];
-        out[e] = make_double2((double)v.x, (double)v.y);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e0 = (long long)blockIdx.x * blockDim.x + threadIdx.x; e0 < n2;
+         e0 += stride * CONVERT_ITEMS) {
+        float2 v[CONVERT_ITEMS];
+#pragma unroll
+        for (int k = 0; k < CONVERT_ITEMS; k++)
+            if (e0 + k * stride < n2) v[k] = in[e0 + k * stride];
+#pragma unroll
+        for (int k = 0; k < CONVERT_ITEMS; k++)
+            if (e0 + k * stride < n2) out[e0 + k * stride] = make_double2((double)v[k].x, (double)v[k].y);
     }
 }
 
@@ -1048,7 +1065,7 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
 static int grid_f64_to_f32(se_batch b, const double* grid, cudaStream_t st)
 {
     const long long n2 = (b->grid_elems + 1) / 2;
-    k_grid_to_f32<<<std::min<long long>(4096, ceil_div(n2, 256)), 256, 0, st>>>(
+    k_grid_to_f32<<<std::min<long long>(CONVERT_CTAS, ceil_div(n2, 256 * CONVERT_ITEMS)), 256, 0, st>>>(
         reinterpret_cast<const double2*>(grid), reinterpret_cast<float2*>(b->grid32), n2);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
@@ -1058,7 +1075,7 @@ static int grid_f64_to_f32(se_batch b, const double* grid, cudaStream_t st)
 static int grid_f32_to_f64(se_batch b, double* grid, cudaStream_t st)
 {
     const long long n2 = (b->grid_elems + 1) / 2;
-    k_grid_to_f64<<<std::min<long long>(4096, ceil_div(n2, 256)), 256, 0, st>>>(
+    k_grid_to_f64<<<std::min<long long>(CONVERT_CTAS, ceil_div(n2, 256 * CONVERT_ITEMS)), 256, 0, st>>>(
         reinterpret_cast<const float2*>(b->grid32), reinterpret_cast<double2*>(grid), n2);
     SE_CUDA(cudaGetLastError());
     LAUNCHED(b);
