@@ -98,6 +98,20 @@ def test_c3_batch_fp64_matches_oracle(env, c3):
         se.close()
 
 
+def test_c3_batch_fp32_equals_single_solves(env, c3):
+    """The batch's 16,384 tiles outnumber 4 CTAs per SM, so its FP32 spread
+    runs the 5-CTA build of k_spread2; one of its systems alone (64 tiles)
+    runs the 4-CTA build.  Both sum in the same order: the same bits."""
+    torch, S, _ = env
+    allsys, systems, xs, qs, outs = c3
+    for i in c3_sample(allsys):
+        s = systems[i]
+        se = S.SpectralEwald(s.M, s.P, s.L, s.xi, None, "potential", "fp32", s.N)
+        one = host(se.solve(torch.tensor(xs[i], device="cuda"), torch.tensor(qs[i], device="cuda")))
+        np.testing.assert_array_equal(outs["fp32"][i], one)
+        se.close()
+
+
 def test_c3_batch_fp32_every_system(env, c3):
     import oracle as O
     allsys, systems, xs, qs, outs = c3
