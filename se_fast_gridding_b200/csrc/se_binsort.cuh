@@ -27,8 +27,8 @@
 constexpr int BSORT_THREADS = 512;
 constexpr int BSORT_MAX_KEYS = 8192;
 constexpr int BSORT_MAX_N = 1 << 19;
-constexpr int BSORT_MAX_CHUNKS = 148;
-constexpr int BSORT_MIN_CHUNK = 512;
+constexpr int BSORT_MAX_CHUNKS = 296;
+constexpr int BSORT_MIN_CHUNK = 256;
 
 // Particles per chunk for ntot particles: at least BSORT_MIN_CHUNK, at most
 // BSORT_MAX_CHUNKS chunks, a multiple of 32.

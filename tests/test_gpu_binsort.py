@@ -33,7 +33,7 @@ def positions(W, N, L, seed, kind):
     (100, 32, 8, "uniform"),          # one chunk
     (5000, 64, 16, "clustered"),      # long runs of equal keys
     (7000, 48, 12, "outside"),
-    (400000, 64, 16, "uniform"),      # 148 chunks of more than the minimum
+    (400000, 64, 16, "uniform"),      # the most chunks, each above the minimum
 ])
 def test_bin_sort_equals_radix_sort(env, prec, N, M, P, kind):
     torch, S, W, L = env
