@@ -18,7 +18,9 @@
 // weights in the working precision; the lanes' sums are reduced in FP64 with
 // shuffles (the four FORCE sums of the FP32 kernel together, warp_sum4).
 // FP32 warps on x rows copy the next particle's record and factor rows into
-// shared memory by cp.async while they sum the current one.
+// shared memory by cp.async while they sum the current one; warps on columns
+// load a particle's three factor rows whole, entry l in lane l, beside its
+// record, and take the factors from the loading lanes by shuffles.
 //
 // Shared-memory pitches (row Ep, plane PL) come from the host, chosen so that
 // the pair loads of one instruction fall in distinct banks.

@@ -4,15 +4,22 @@
 // plan is a batch of one); per-system parameters and offsets live in a small
 // device table (SysDev).
 //
-//   k_prepare   per particle: stencil corner and offset as fgg_expansion_3p
-//               (SE_fgg.c:539-621), charge x d, fine-bin key
-//   stable_sort by fine-bin key (se_sort.cu), then k_gather into bin order
+//   sort        per particle the stencil corner and offset as fgg_expansion_3p
+//               (SE_fgg.c:539-621), charge x d and fine-bin key, then the
+//               stable counting sort into bin order: k_bsort_count /
+//               _columns / _scatter (se_binsort.cuh) for batches of at most
+//               8192 bins and 2^19 particles, else k_prepare, the radix sort
+//               of se_sort.cu and k_gather
 //   k_factors   each particle's separable Gaussian factors, FGG recurrence
-//   k_spread    one CTA per output tile of the periodic grid, the fold fused
-//               (se_spread.cuh)
+//               (tile-aligned rows for the tile kernels)
+//   spread      k_tile_parts + k_spread2, one CTA per part of a 16^3 tile,
+//               the fold fused (se_spread2.cuh), for grids of whole tiles and
+//               P <= 16; k_spread (se_spread.cuh) for the others
 //   cuFFT D2Z, k_scale (Z of scaling(), SE_general.c:145-175, applied to the
 //               half spectrum as product_rc does, SE_general.c:336-362), Z2D
-//   k_interp    one CTA per fine bin, the unfold fused (se_interp.cuh)
+//   interp      k_grid_to_f32 (FP32 path) + k_interp2, one CTA per fine bin,
+//               the unfold fused (se_interp2.cuh), beside k_spread2;
+//               k_interp (se_interp.cuh) for the others
 //
 // Grid layout: M^3 FP64 row-major [x][y][z], the transpose of the reference's
 // column-major H_per; the FFT of the transpose is the transpose of the FFT and
