@@ -123,6 +123,11 @@ int se_plan_destroy(se_plan plan);
  * Off by default: on B200 it ties cuFFT on one M = 128 grid and is slower on
  * batches of many M = 64 grids. */
 #define SE_PATH_FFT3 16
+/* Stage one window per fine bin in the pair interpolation instead of one per
+ * two z-adjacent bins (the FP32 default where the larger window fits three
+ * CTAs per SM); both sum the same cells in the same order, so the results
+ * are identical. */
+#define SE_PATH_BIN_WINDOWS 32
 int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path);
 /* The path the default choice gives a system of grid M and stencil P. */
 int se_default_path(int M, int P);

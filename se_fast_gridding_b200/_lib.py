@@ -90,6 +90,7 @@ SE_WHERE_HOST, SE_WHERE_DEVICE = 0, 1
 SE_PATH_DEFAULT, SE_PATH_TUNE = -1, -2
 SE_PATH_TILE_SPREAD, SE_PATH_PAIR_INTERP, SE_PATH_RUNTIME_P, SE_PATH_RADIX_SORT = 1, 2, 4, 8
 SE_PATH_FFT3 = 16
+SE_PATH_BIN_WINDOWS = 32
 SE_POTENTIAL, SE_FORCE = 0, 1
 SE_FP64, SE_FP32, SE_FP32_FFT32 = 0, 1, 2
 

@@ -38,6 +38,7 @@ constexpr int PATH_PAIR_INTERP = 2;    // k_interp2 (else k_interp / k_interp_gl
 constexpr int PATH_RUNTIME_P = 4;      // interpolation without the P-unrolled variants
 constexpr int PATH_RADIX_SORT = 8;     // the batch sorts with the radix passes (se_sort.cu)
 constexpr int PATH_FFT3 = 16;          // the batch's FP64 FFTs through se_fft.cuh (not cuFFT)
+constexpr int PATH_BIN_WINDOWS = 32;   // k_interp2 stages one window per bin (not per z pair)
 
 // The default path: the tile-aligned spread wherever it applies, and the
 // window-pair interpolation from P = 8 on (for shorter stencils its

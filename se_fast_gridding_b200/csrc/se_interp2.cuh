@@ -4,8 +4,11 @@
 // tiles, P <= 16).  Included inside namespace se by se_solve.cu after
 // se_interp.cuh.
 //
-// One CTA per fine bin (8^3 stencil corners).  The bin's window, E = 7 + P
-// cells per axis in x and y and EZ = 8 + P rounded up to 4 in z, is copied
+// One CTA per fine bin (8^3 stencil corners), or per pair of z-adjacent
+// bins where bins are sparse and the larger window still leaves three CTAs
+// per SM (FP32).  The
+// window, E = 7 + P cells per axis in x and y and EZ = 8 zb + P rounded up
+// to 4 in z (zb = 1 or 2 bins), is copied
 // from the grid (a FP32 copy of it on the FP32 path) by cp.async, a 4-cell
 // group at a time: the window starts on a multiple of 8 in every axis and M
 // is a multiple of 16, so every group is contiguous even where the window
@@ -26,6 +29,9 @@
 // the pair loads of one instruction fall in distinct banks.
 
 constexpr int I2_WARPS = 8;
+#ifndef SE_I2_ZMERGE
+#define SE_I2_ZMERGE 1   // windows of two z-adjacent bins where they fit
+#endif
 
 template <typename T>
 struct Interp2Warp {
@@ -86,8 +92,9 @@ __device__ __forceinline__ void warp_sum4(double& v0, double& v1, double& v2, do
     v3 = __shfl_sync(0xffffffffu, u, 24);
 }
 
-// z extent of the staged window: the pairs of any stencil start r2 < 8 fit.
-__host__ __device__ constexpr int interp2_ez(int P) { return (8 + P + 3) & ~3; }
+// z extent of the staged window of zb z-adjacent bins: the pairs of any
+// stencil start r2 < 8 zb fit.
+__host__ __device__ constexpr int interp2_ez(int P, int zb = 1) { return (FB * zb + P + 3) & ~3; }
 
 // FP32 rows of x (interp2_rows_f32): the next particle's record, packed
 // corner, input index and factor rows, copied by cp.async into a per-warp
@@ -294,30 +301,38 @@ __device__ __forceinline__ void interp2_columns(
 
 // FORCE: the force weights and sums are computed (every system of a batch
 // with a FORCE system runs this variant; each stores what its mode asks).
+// zb = 2: the CTA of a bin with an even z index also takes its z neighbour
+// (the next bin: nf[2] is even for these systems), so one window of
+// 7 + P x 7 + P x 16 + P cells serves the particles of both, and the CTA of
+// the odd bin returns at once.  Each particle sums the same window cells in
+// the same pairs either way (its offset in the window moves by 8 cells in
+// z), so the results do not depend on zb.
 template <typename T, int PT, bool FORCE>
 __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_interp2(
     const SysDev* __restrict__ sys, const int* __restrict__ bin_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const int* __restrict__ sperm, const T* __restrict__ rows, const int* __restrict__ boff,
     const T* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out,
-    int Ep, int PL)
+    int Ep, int PL, int zb)
 {
     using PV = Pair<T>;
     using VT = typename PV::V;
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ Interp2Warp<T> wsm[I2_WARPS];
     const int bin = blockIdx.x;
-    const int beg = boff[bin], end = boff[bin + 1];
-    if (beg == end) return;
     const SysDev& S = sys[find_sys(bin_prefix, nsys, bin)];
     if (!(S.path & PATH_PAIR_INTERP)) return;   // k_interp covers this system
+    const int lb = bin - S.bin_base;
+    // (nf[2] even: the parity of lb is that of the bin's z index)
+    if (zb == 2 && (lb & 1)) return;
+    const int beg = boff[bin], end = boff[bin + zb];
+    if (beg == end) return;
     const int P = PT ? PT : S.P;
     const int M = S.M;
-    const int lb = bin - S.bin_base;
     const int o0 = (lb / (S.nf[1] * S.nf[2])) * FB;
     const int o1 = ((lb / S.nf[2]) % S.nf[1]) * FB;
     const int o2 = (lb % S.nf[2]) * FB;
-    const int E = FB + P - 1, EZ = interp2_ez(P);
+    const int E = FB + P - 1, EZ = interp2_ez(P, zb);
     T* tile = reinterpret_cast<T*>(dsm);
     const T* gs = grid + S.grid_off;
     const int warp = threadIdx.x >> 5;

@@ -424,6 +424,7 @@ struct se_batch_s {
     int i2_P = 0;             // largest P of the k_interp2 systems (0: none)
     bool i2_uniform = false;  // all k_interp2 systems have P == i2_P
     int i2_Ep = 0, i2_PL = 0; // k_interp2 window pitches
+    int i2_zb = 1;            // z-adjacent bins per k_interp2 window (1 or 2)
     size_t i2_smem = 0;
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
@@ -675,13 +676,16 @@ static cudaError_t raise_smem_limit(const void* fn, size_t smem)
 }
 
 // Row pitch Ep and plane pitch PL (elements, both even) of k_interp2's
-// window for stencils up to P: the pair loads of one warp instruction are
-// served in 128-byte groups of lanes; count, over all load rounds m, the
-// largest number of distinct 4-byte words that share a bank within a group,
-// and keep the smallest.
-static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
+// window of zb z-adjacent bins for stencils up to P: the pair loads of one
+// warp instruction are served in 128-byte groups of lanes; count, over all
+// load rounds m, the largest number of distinct 4-byte words that share a
+// bank within a group, and keep the smallest among the windows of at most
+// cap_bytes.  Returns false (and the smallest window) when none fits.
+static bool interp2_pitch(int P, int precision, int zb, size_t cap_bytes, int* Ep_out,
+                          int* PL_out)
 {
-    const int E = FB + P - 1, EZ = interp2_ez(P);
+    const int E = FB + P - 1, EZ = interp2_ez(P, zb);
+    const size_t elem = precision == SE_FP32 ? 4 : 8;
     const int words = precision == SE_FP32 ? 2 : 4;   // 4-byte words per pair
     const int group = 32 / words;                     // lanes per 128 bytes
     // the lanes' (x, y) columns per load round: FP32 with P not dividing 32
@@ -707,6 +711,7 @@ static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
     for (int Ep = EZ; Ep <= EZ + 32; Ep += 2) {
         for (int pad = 0; pad <= 64; pad += 2) {
             const int PL = E * Ep + pad;
+            if ((size_t)E * PL * elem > cap_bytes) continue;
             int cost = 0;
             for (int m = 0; m < rounds; m++) {
                 for (int g0 = 0; g0 < 32; g0 += group) {
@@ -737,6 +742,56 @@ static void interp2_pitch(int P, int precision, int* Ep_out, int* PL_out)
     }
     *Ep_out = best_Ep;
     *PL_out = best_PL;
+    return best_cost < (1 << 30);
+}
+
+template <typename T, bool FORCE>
+static const void* interp2_kernel(int P, bool uniform)
+{
+    return (uniform && P == 8)    ? (const void*)k_interp2<T, 8, FORCE>
+           : (uniform && P == 12) ? (const void*)k_interp2<T, 12, FORCE>
+           : (uniform && P == 16) ? (const void*)k_interp2<T, 16, FORCE>
+                                  : (const void*)k_interp2<T, 0, FORCE>;
+}
+
+// The k_interp2 window of a batch: two z-adjacent bins per window where the
+// bins are sparse (at most I2_ZMERGE_MEAN particles per bin on average) and
+// that window (beside the kernel's static shared memory) still leaves the
+// CTAs per SM its launch bounds ask for (FP32: 3), else one bin.  Measured on
+// B200: 100,000 particles in 4,096 bins (M = 128, P = 16) 0.139 -> 0.123 ms;
+// 16M clustered particles in 262,144 bins (M = 512, P = 12) 11.3 -> 11.7 ms,
+// where a window's copy is a small share of its particles' work and CTAs of
+// two crowded bins lengthen the tail.
+constexpr int I2_ZMERGE_MEAN = 32;
+static int interp2_window(se_batch_s* b, bool any_force)
+{
+    const bool fp32 = b->precision == SE_FP32;
+    const bool u = b->i2_uniform && !b->runtime_p;
+    const void* fn = fp32 ? (any_force ? interp2_kernel<float, true>(b->i2_P, u)
+                                       : interp2_kernel<float, false>(b->i2_P, u))
+                          : (any_force ? interp2_kernel<double, true>(b->i2_P, u)
+                                       : interp2_kernel<double, false>(b->i2_P, u));
+    cudaFuncAttributes fa;
+    SE_CUDA(cudaFuncGetAttributes(&fa, fn));
+    int dev = 0, sm_bytes = 0, reserved = 0;
+    SE_CUDA(cudaGetDevice(&dev));
+    SE_CUDA(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    SE_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    const int ctas = fp32 ? 3 : 2;
+    const long long cap = (long long)sm_bytes / ctas - reserved - (long long)fa.sharedSizeBytes;
+    const size_t capb = cap > 0 ? (size_t)cap : 0;
+    bool bin_windows = false;
+    for (const auto& S : b->host_sys)
+        if ((S.path & PATH_PAIR_INTERP) && (S.path & PATH_BIN_WINDOWS)) bin_windows = true;
+    const bool sparse = (long long)b->ntot <= (long long)I2_ZMERGE_MEAN * b->nbins;
+    b->i2_zb = 1;
+    if (SE_I2_ZMERGE && fp32 && sparse && !bin_windows &&
+        interp2_pitch(b->i2_P, b->precision, 2, capb, &b->i2_Ep, &b->i2_PL))
+        b->i2_zb = 2;
+    else
+        interp2_pitch(b->i2_P, b->precision, 1, capb, &b->i2_Ep, &b->i2_PL);
+    b->i2_smem = (size_t)(FB + b->i2_P - 1) * b->i2_PL * (fp32 ? 4 : 8);
+    return SE_OK;
 }
 
 static int batch_create(se_batch* out, const se_system* systems, int nsys, int precision,
@@ -750,7 +805,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     for (int i = 0; i < nsys; i++) {
         if (!valid_system(systems[i])) return SE_ERR_INVALID;
         const int path = path_of(systems, paths, i);
-        if (path < 0 || path > 31 ||
+        if (path < 0 || path > 63 ||
             ((path & (PATH_TILE_SPREAD | PATH_PAIR_INTERP)) &&
              !spread2_eligible(systems[i].M, systems[i].P)))
             return SE_ERR_INVALID;
@@ -884,8 +939,12 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
             if (b->i2_P && systems[i].P != b->i2_P) b->i2_uniform = false;
             b->i2_P = std::max(b->i2_P, systems[i].P);
         }
-        interp2_pitch(b->i2_P, precision, &b->i2_Ep, &b->i2_PL);
-        b->i2_smem = (size_t)(FB + b->i2_P - 1) * b->i2_PL * (precision == SE_FP32 ? 4 : 8);
+        bool i2_force = false;
+        for (int i = 0; i < nsys; i++)
+            if ((b->host_sys[i].path & PATH_PAIR_INTERP) && b->host_sys[i].mode == SE_FORCE)
+                i2_force = true;
+        const int rc = interp2_window(b, i2_force);
+        if (rc != SE_OK) return fail(rc);
     }
     b->bsort = bsort_fits(b->ntot, b->nbins);
     for (int i = 0; i < nsys; i++)
@@ -1040,12 +1099,12 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
         LAUNCHED(b);
         if (b->precision == SE_FP32)
             (b->spread2_few ? k_spread2<float, S2_BLOCKS_FEW> : k_spread2<float, S2_BLOCKS_MANY>)
-                <<<bound, S2_THREADS, 0, st>>>(
+                <<<bound * S2_CTA_SPLIT, S2_THREADS, 0, st>>>(
                     b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
                     static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
                     b->tile_done, b->slab, b->slab_slots, b->err);
         else
-            k_spread2<double, S2_BLOCKS_FP64><<<bound, S2_THREADS, 0, st>>>(
+            k_spread2<double, S2_BLOCKS_FP64><<<bound * S2_CTA_SPLIT, S2_THREADS, 0, st>>>(
                 b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
                 static_cast<const double*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
                 b->tile_done, b->slab, b->slab_slots, b->err);
@@ -1215,15 +1274,12 @@ static int launch_interp2_mode(se_batch b, const T* grid, double* out, double* p
 {
     const int P = b->i2_P;
     const bool u = b->i2_uniform && !b->runtime_p;
-    const void* fn = (u && P == 8)    ? (const void*)k_interp2<T, 8, FORCE>
-                     : (u && P == 12) ? (const void*)k_interp2<T, 12, FORCE>
-                     : (u && P == 16) ? (const void*)k_interp2<T, 16, FORCE>
-                                      : (const void*)k_interp2<T, 0, FORCE>;
+    const void* fn = interp2_kernel<T, FORCE>(P, u);
     SE_CUDA(raise_smem_limit(fn, b->i2_smem));
     const dim3 grd(std::max(b->nbins, 1)), blk(I2_WARPS * 32);
     const T* rows = static_cast<const T*>(b->rows);
 #define SE_I2ARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, rows, b->boff, grid, \
-                  out, phi, b->i2_Ep, b->i2_PL
+                  out, phi, b->i2_Ep, b->i2_PL, b->i2_zb
     if (u && P == 8) k_interp2<T, 8, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
     else if (u && P == 12) k_interp2<T, 12, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
     else if (u && P == 16) k_interp2<T, 16, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
@@ -1667,7 +1723,7 @@ extern "C" int se_plan_create_ex(se_plan* plan, const se_config* cfg, int path)
                              cfg->precision != SE_FP32_FFT32))
         return SE_ERR_INVALID;
     if (path == SE_PATH_TUNE) SE_TRY(tune_path(cfg, &path));
-    if (path < 0 || path > 31) return SE_ERR_INVALID;
+    if (path < 0 || path > 63) return SE_ERR_INVALID;
     se_plan p = new se_plan_s();
     p->cfg = *cfg;
     const int r = batch_create(&p->b, &s, 1, cfg->precision, &path);

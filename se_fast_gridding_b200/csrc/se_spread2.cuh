@@ -52,8 +52,18 @@
 #define SE_S2_UNROLL 16
 #endif
 constexpr int S2_CAP = SE_S2_CAP;   // candidates per part of a warp's list
-constexpr int S2_WARPS = 4;
-constexpr int S2_THREADS = S2_WARPS * 32;
+constexpr int S2_WARPS = 4;   // warp blocks per tile
+// warps per CTA: a tile's four warp blocks run as S2_WARPS / S2_CTA_WARPS
+// CTAs (the warps are independent), so that the SMs share out the blocks
+// more evenly (two CTAs of 2 warps per tile against one of 4: C2 spread
+// 0.135 -> 0.128 ms, C3 2.33 -> 2.26 ms, C5 12.7 -> 11.6 ms)
+#ifndef SE_S2_CTA_WARPS
+#define SE_S2_CTA_WARPS 2
+#endif
+constexpr int S2_CTA_WARPS = SE_S2_CTA_WARPS;
+constexpr int S2_CTA_SPLIT = S2_WARPS / S2_CTA_WARPS;   // CTAs per part of a tile
+constexpr int S2_THREADS = S2_CTA_WARPS * 32;
+static_assert(S2_WARPS % S2_CTA_WARPS == 0, "a tile's warp blocks split evenly into CTAs");
 constexpr int S2_LIST = 64;    // per-class list ring: >= group - 1 + 32
 constexpr int S2_SEGS = 64;    // bin segments reaching a warp's block: <= 5 x 4 x 2 for P <= 16
 constexpr int S2_FOLD = 512;   // FP32 partial sums cover this many of a warp's particles
@@ -80,10 +90,10 @@ struct Spread2Stage {
 
 template <typename Acc>
 struct Spread2Smem {
-    Spread2Stage<Acc> stage[S2_WARPS][2];
-    int2 list[S2_WARPS][S2_CLASSES][S2_LIST];   // (particle, packed grid index)
-    int seg_beg[S2_WARPS][S2_SEGS];
-    int seg_pre[S2_WARPS][S2_SEGS];
+    Spread2Stage<Acc> stage[S2_CTA_WARPS][2];
+    int2 list[S2_CTA_WARPS][S2_CLASSES][S2_LIST];   // (particle, packed grid index)
+    int seg_beg[S2_CTA_WARPS][S2_SEGS];
+    int seg_pre[S2_CTA_WARPS][S2_SEGS];
 };
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc)
@@ -350,7 +360,7 @@ __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
 }
 
 template <typename Acc, int BLOCKS>
-__global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
+__global__ void __launch_bounds__(S2_THREADS, BLOCKS * S2_CTA_SPLIT) k_spread2(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid,
@@ -364,7 +374,8 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
     __shared__ int folds;   // this CTA finished its tile's parts last
 
     // ---- the part this CTA sums: tile = the last t with tile_parts[t] <= item
-    const int item = blockIdx.x;
+    // (warp blocks sub S2_CTA_WARPS + [0, S2_CTA_WARPS) of it)
+    const int item = blockIdx.x / S2_CTA_SPLIT, sub = blockIdx.x % S2_CTA_SPLIT;
     if (item >= tile_parts[ntiles]) return;
     int tile = 0;
     {
@@ -388,7 +399,8 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
     const int lt = tile - S.tile_base;
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
     const int x0 = tix * 16, y0 = tiy * 16, z0 = tiz * 16;
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int t = threadIdx.x, lw = t >> 5, lane = t & 31;
+    const int warp = sub * S2_CTA_WARPS + lw;   // the warp block of the tile
     const int wy = warp >> 1, wz = warp & 1;
     const int ly = lane >> 2, lz = (lane & 3) * 2;
     const unsigned ybits = 0xFFu << (8 * wy), zbits = 0xFFu << (8 * wz);
@@ -401,8 +413,8 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
         if (lane == 0) atomicOr(err, 2);
         nseg = 0;
     }
-    int* seg_beg = sm.seg_beg[warp];
-    int* seg_pre = sm.seg_pre[warp];
+    int* seg_beg = sm.seg_beg[lw];
+    int* seg_pre = sm.seg_pre[lw];
     int total = 0;
     for (int u0 = 0; u0 < nseg; u0 += 32) {
         const int u = u0 + lane;
@@ -472,7 +484,7 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
             if (cls >= 0) {
                 const unsigned kc = cls == 0 ? k0 : (cls == 1 ? k1 : k2);
                 const int sh = 8 * cls;
-                sm.list[warp][cls][((ring >> sh) + (cnt >> sh) + __popc(kc & lanes_before)) &
+                sm.list[lw][cls][((ring >> sh) + (cnt >> sh) + __popc(kc & lanes_before)) &
                                    (S2_LIST - 1)] = make_int2(part, pk);
             }
             cnt += __popc(k0) | (__popc(k1) << 8) | (__popc(k2) << 16);
@@ -487,12 +499,12 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
         const int sh = 8 * cls;
         const int avail = (cnt >> sh) & 0xFF;
         const int head = (ring >> sh) & (S2_LIST - 1);
-        const int2* list = sm.list[warp][cls];
+        const int2* list = sm.list[lw][cls];
         // ---- stage the next group of the class: lane l < n copies its
         // particle head + l (of a one-half class, that half of the x row)
         const int n = min(G, avail);
         if (n > 0) {
-            Spread2Stage<Acc>& st = sm.stage[warp][buf];
+            Spread2Stage<Acc>& st = sm.stage[lw][buf];
             if (lane < n) {
                 const int2 e = list[(head + lane) & (S2_LIST - 1)];
                 const int hx = tile_half(g_of(e.y, 0), tix, nt, P);
@@ -531,7 +543,7 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
             if (n > 0) cp_async_wait<1>();
             else cp_async_wait<0>();
             __syncwarp();
-            Spread2Stage<Acc>& st = sm.stage[warp][buf ^ 1];
+            Spread2Stage<Acc>& st = sm.stage[lw][buf ^ 1];
             // lane i scales its particle's 8 y entries by the charge, once
             if (lane < pending) {
                 const Acc qv = (Acc)st.q[lane];
@@ -589,7 +601,7 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS) k_spread2(
     if (nparts > 1) {
         __threadfence();
         __syncthreads();
-        if (t == 0) folds = atomicAdd(&tile_done[tile], 1) == nparts - 1;
+        if (t == 0) folds = atomicAdd(&tile_done[tile], 1) == nparts * S2_CTA_SPLIT - 1;
         __syncthreads();
         if (folds) {
             __threadfence();

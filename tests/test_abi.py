@@ -135,4 +135,4 @@ def test_path_constants_match_the_header():
     for name, value in defs.items():
         assert getattr(_lib, name) == int(value), name
     assert {"SE_PATH_TILE_SPREAD", "SE_PATH_PAIR_INTERP", "SE_PATH_RUNTIME_P",
-            "SE_PATH_RADIX_SORT", "SE_PATH_FFT3"} <= set(defs)
+            "SE_PATH_RADIX_SORT", "SE_PATH_FFT3", "SE_PATH_BIN_WINDOWS"} <= set(defs)
