@@ -301,6 +301,8 @@ __device__ __forceinline__ void interp2_columns(
 
 // FORCE: the force weights and sums are computed (every system of a batch
 // with a FORCE system runs this variant; each stores what its mode asks).
+// pfilter: the stencil of the systems this launch serves (0: all); a batch
+// of several stencils runs one launch per stencil, each with its window.
 // zb = 2: the CTA of a bin with an even z index also takes its z neighbour
 // (the next bin: nf[2] is even for these systems), so one window of
 // 7 + P x 7 + P x 16 + P cells serves the particles of both, and the CTA of
@@ -313,7 +315,7 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const int* __restrict__ sperm, const T* __restrict__ rows, const int* __restrict__ boff,
     const T* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out,
-    int Ep, int PL, int zb)
+    int Ep, int PL, int zb, int pfilter)
 {
     using PV = Pair<T>;
     using VT = typename PV::V;
@@ -322,6 +324,7 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     const int bin = blockIdx.x;
     const SysDev& S = sys[find_sys(bin_prefix, nsys, bin)];
     if (!(S.path & PATH_PAIR_INTERP)) return;   // k_interp covers this system
+    if (pfilter && S.P != pfilter) return;      // another launch's stencil
     const int lb = bin - S.bin_base;
     // (nf[2] even: the parity of lb is that of the bin's z index)
     if (zb == 2 && (lb & 1)) return;

@@ -421,11 +421,19 @@ struct se_batch_s {
     float* grid32 = nullptr;  // FP32 copy of the grids, staged by k_interp2<float>
     bool fft32 = false;       // SE_FP32_FFT32: FP32 FFTs on grid32 / spec32
     float2* spec32 = nullptr;
-    int i2_P = 0;             // largest P of the k_interp2 systems (0: none)
-    bool i2_uniform = false;  // all k_interp2 systems have P == i2_P
-    int i2_Ep = 0, i2_PL = 0; // k_interp2 window pitches
-    int i2_zb = 1;            // z-adjacent bins per k_interp2 window (1 or 2)
-    size_t i2_smem = 0;
+    // k_interp2 launches: one per stencil P of its systems (P-specialised
+    // kernels where they exist), or one runtime-P launch over all of them
+    // when some system asks for runtime P; each with its own window
+    struct I2Class {
+        int P = 0;              // the systems it serves (0: all, runtime P)
+        int Pw = 0;             // the stencil its window is sized for
+        bool special = false;   // the P-specialised kernel
+        int Ep = 0, PL = 0;     // window pitches
+        int zb = 1;             // z-adjacent bins per window (1 or 2)
+        size_t smem = 0;
+    };
+    std::vector<I2Class> i2_cls;
+    bool i2_force = false;    // some k_interp2 system is in FORCE mode
     void* sort_scratch = nullptr;
     size_t sort_bytes = 0;
     bool bsort = false;   // the three-kernel bin sort (se_binsort.cuh) fits
@@ -746,13 +754,15 @@ static bool interp2_pitch(int P, int precision, int zb, size_t cap_bytes, int* E
 }
 
 template <typename T, bool FORCE>
-static const void* interp2_kernel(int P, bool uniform)
+static const void* interp2_kernel(int P, bool special)
 {
-    return (uniform && P == 8)    ? (const void*)k_interp2<T, 8, FORCE>
-           : (uniform && P == 12) ? (const void*)k_interp2<T, 12, FORCE>
-           : (uniform && P == 16) ? (const void*)k_interp2<T, 16, FORCE>
+    return (special && P == 8)    ? (const void*)k_interp2<T, 8, FORCE>
+           : (special && P == 12) ? (const void*)k_interp2<T, 12, FORCE>
+           : (special && P == 16) ? (const void*)k_interp2<T, 16, FORCE>
                                   : (const void*)k_interp2<T, 0, FORCE>;
 }
+
+static bool interp2_special(int P) { return P == 8 || P == 12 || P == 16; }
 
 // The k_interp2 window of a batch: two z-adjacent bins per window where the
 // bins are sparse (at most I2_ZMERGE_MEAN particles per bin on average) and
@@ -763,14 +773,15 @@ static const void* interp2_kernel(int P, bool uniform)
 // where a window's copy is a small share of its particles' work and CTAs of
 // two crowded bins lengthen the tail.
 constexpr int I2_ZMERGE_MEAN = 32;
-static int interp2_window(se_batch_s* b, bool any_force)
+static int interp2_window(const se_batch_s* b, se_batch_s::I2Class& c, long long nparticles,
+                          long long nbins, bool bin_windows)
 {
     const bool fp32 = b->precision == SE_FP32;
-    const bool u = b->i2_uniform && !b->runtime_p;
-    const void* fn = fp32 ? (any_force ? interp2_kernel<float, true>(b->i2_P, u)
-                                       : interp2_kernel<float, false>(b->i2_P, u))
-                          : (any_force ? interp2_kernel<double, true>(b->i2_P, u)
-                                       : interp2_kernel<double, false>(b->i2_P, u));
+    const bool force = b->i2_force;
+    const void* fn = fp32 ? (force ? interp2_kernel<float, true>(c.Pw, c.special)
+                                   : interp2_kernel<float, false>(c.Pw, c.special))
+                          : (force ? interp2_kernel<double, true>(c.Pw, c.special)
+                                   : interp2_kernel<double, false>(c.Pw, c.special));
     cudaFuncAttributes fa;
     SE_CUDA(cudaFuncGetAttributes(&fa, fn));
     int dev = 0, sm_bytes = 0, reserved = 0;
@@ -780,17 +791,54 @@ static int interp2_window(se_batch_s* b, bool any_force)
     const int ctas = fp32 ? 3 : 2;
     const long long cap = (long long)sm_bytes / ctas - reserved - (long long)fa.sharedSizeBytes;
     const size_t capb = cap > 0 ? (size_t)cap : 0;
-    bool bin_windows = false;
-    for (const auto& S : b->host_sys)
-        if ((S.path & PATH_PAIR_INTERP) && (S.path & PATH_BIN_WINDOWS)) bin_windows = true;
-    const bool sparse = (long long)b->ntot <= (long long)I2_ZMERGE_MEAN * b->nbins;
-    b->i2_zb = 1;
+    const bool sparse = nparticles <= (long long)I2_ZMERGE_MEAN * nbins;
+    c.zb = 1;
     if (SE_I2_ZMERGE && fp32 && sparse && !bin_windows &&
-        interp2_pitch(b->i2_P, b->precision, 2, capb, &b->i2_Ep, &b->i2_PL))
-        b->i2_zb = 2;
-    else
-        interp2_pitch(b->i2_P, b->precision, 1, capb, &b->i2_Ep, &b->i2_PL);
-    b->i2_smem = (size_t)(FB + b->i2_P - 1) * b->i2_PL * (fp32 ? 4 : 8);
+        interp2_pitch(c.Pw, b->precision, 2, capb, &c.Ep, &c.PL))
+        c.zb = 2;
+    else   // one bin: the least conflicted pitch, whatever its size (the
+           // pitch is worth more than a CTA per SM: FP64 P = 16 at the
+           // smallest pitch that fits two CTAs ran 1.5x slower)
+        interp2_pitch(c.Pw, b->precision, 1, (size_t)-1, &c.Ep, &c.PL);
+    c.smem = (size_t)(FB + c.Pw - 1) * c.PL * (fp32 ? 4 : 8);
+    return SE_OK;
+}
+
+// The k_interp2 launches of a batch (se_batch_s::i2_cls).
+static int interp2_classes(se_batch_s* b, const se_system* systems, int nsys)
+{
+    std::map<int, std::pair<long long, long long>> byP;   // P -> (particles, bins)
+    bool bin_windows = false;
+    int maxP = 0;
+    long long np = 0, nb = 0;
+    for (int i = 0; i < nsys; i++) {
+        const SysDev& S = b->host_sys[i];
+        if (!(S.path & PATH_PAIR_INTERP)) continue;
+        const long long bins = (long long)S.nf[0] * S.nf[1] * S.nf[2];
+        byP[systems[i].P].first += systems[i].N;
+        byP[systems[i].P].second += bins;
+        np += systems[i].N;
+        nb += bins;
+        maxP = std::max(maxP, systems[i].P);
+        if (S.mode == SE_FORCE) b->i2_force = true;
+        if (S.path & PATH_BIN_WINDOWS) bin_windows = true;
+    }
+    b->i2_cls.clear();
+    if (b->runtime_p) {
+        se_batch_s::I2Class c;
+        c.P = 0;
+        c.Pw = maxP;
+        SE_TRY(interp2_window(b, c, np, nb, bin_windows));
+        b->i2_cls.push_back(c);
+        return SE_OK;
+    }
+    for (const auto& kv : byP) {
+        se_batch_s::I2Class c;
+        c.P = c.Pw = kv.first;
+        c.special = interp2_special(kv.first);
+        SE_TRY(interp2_window(b, c, kv.second.first, kv.second.second, bin_windows));
+        b->i2_cls.push_back(c);
+    }
     return SE_OK;
 }
 
@@ -933,17 +981,7 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
         SE_ALLOC(b->grid32, sizeof(float) * (b->grid_elems + 16));
     if (fft32) SE_ALLOC(b->spec32, sizeof(float2) * b->spec_elems);
     if (b->any_interp2) {
-        b->i2_uniform = true;
-        for (int i = 0; i < nsys; i++) {
-            if (!(b->host_sys[i].path & PATH_PAIR_INTERP)) continue;
-            if (b->i2_P && systems[i].P != b->i2_P) b->i2_uniform = false;
-            b->i2_P = std::max(b->i2_P, systems[i].P);
-        }
-        bool i2_force = false;
-        for (int i = 0; i < nsys; i++)
-            if ((b->host_sys[i].path & PATH_PAIR_INTERP) && b->host_sys[i].mode == SE_FORCE)
-                i2_force = true;
-        const int rc = interp2_window(b, i2_force);
+        const int rc = interp2_classes(b, systems, nsys);
         if (rc != SE_OK) return fail(rc);
     }
     b->bsort = bsort_fits(b->ntot, b->nbins);
@@ -1272,31 +1310,30 @@ template <typename T, bool FORCE>
 static int launch_interp2_mode(se_batch b, const T* grid, double* out, double* phi,
                                cudaStream_t st)
 {
-    const int P = b->i2_P;
-    const bool u = b->i2_uniform && !b->runtime_p;
-    const void* fn = interp2_kernel<T, FORCE>(P, u);
-    SE_CUDA(raise_smem_limit(fn, b->i2_smem));
+    // one launch per class; the CTAs of the other classes' bins return at once
     const dim3 grd(std::max(b->nbins, 1)), blk(I2_WARPS * 32);
     const T* rows = static_cast<const T*>(b->rows);
+    for (const auto& c : b->i2_cls) {
+        const void* fn = interp2_kernel<T, FORCE>(c.Pw, c.special);
+        SE_CUDA(raise_smem_limit(fn, c.smem));
+        const int P = c.special ? c.Pw : 0;
 #define SE_I2ARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, rows, b->boff, grid, \
-                  out, phi, b->i2_Ep, b->i2_PL, b->i2_zb
-    if (u && P == 8) k_interp2<T, 8, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
-    else if (u && P == 12) k_interp2<T, 12, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
-    else if (u && P == 16) k_interp2<T, 16, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
-    else k_interp2<T, 0, FORCE><<<grd, blk, b->i2_smem, st>>>(SE_I2ARGS);
+                  out, phi, c.Ep, c.PL, c.zb, c.P
+        if (P == 8) k_interp2<T, 8, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
+        else if (P == 12) k_interp2<T, 12, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
+        else if (P == 16) k_interp2<T, 16, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
+        else k_interp2<T, 0, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
 #undef SE_I2ARGS
-    SE_CUDA(cudaGetLastError());
-    LAUNCHED(b);
+        SE_CUDA(cudaGetLastError());
+        LAUNCHED(b);
+    }
     return SE_OK;
 }
 
 template <typename T>
 static int launch_interp2(se_batch b, const T* grid, double* out, double* phi, cudaStream_t st)
 {
-    bool any_force = false;
-    for (const auto& S : b->host_sys)
-        if ((S.path & PATH_PAIR_INTERP) && S.mode == SE_FORCE) any_force = true;
-    return any_force ? launch_interp2_mode<T, true>(b, grid, out, phi, st)
+    return b->i2_force ? launch_interp2_mode<T, true>(b, grid, out, phi, st)
                      : launch_interp2_mode<T, false>(b, grid, out, phi, st);
 }
 
