@@ -39,6 +39,13 @@ int stable_sort(const int* keys, const int* vals_in, int N, int nkeys, int* perm
                 int* sorted_keys, int* offsets, void* scratch, size_t scratch_bytes,
                 cudaStream_t st, int* launches);
 
+// ---- copies between pageable host arrays and device memory (se_hoststage.cu):
+// pipelined through pinned chunks, host side split over threads; both return
+// when the data is in place.  device_to_host needs the device work that
+// wrote d finished.
+int host_to_device(void* d, const void* h, size_t bytes);
+int device_to_host(void* h, const void* d, size_t bytes);
+
 // Device flag a plan's kernels set when a position was not finite (reset at
 // the start of each solve on the plan's stream).
 const int* plan_error_flag(se_plan p);

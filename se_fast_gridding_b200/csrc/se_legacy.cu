@@ -8,7 +8,8 @@
 // order of the additions into a grid cell can differ (rounding level).
 //
 // Pointers may be host, pinned, managed or device memory.  Host buffers are
-// staged through cached device mirrors inside each call; managed and device
+// staged through pooled device mirrors inside each call (the copies
+// pipelined through pinned chunks, se_hoststage.cu); managed and device
 // buffers are used in place.  Every call ends with its outputs visible to the
 // host (synchronous, as the reference is).
 #include <cuda_runtime.h>
@@ -17,6 +18,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <iterator>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -69,50 +72,73 @@ static bool on_device(const void* p)
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-struct MirrorCache {
+// Device buffers that stand in for the caller's host arrays during a call.
+// A call takes them from this pool and gives them back when it returns (its
+// outputs are in host memory by then), so a caller that passes new host
+// arrays on every call -- spectral_ewald() mallocs its grids per solve --
+// reuses the same device memory instead of allocating it again.  Idle
+// buffers beyond LIMIT bytes are freed, largest first.
+struct MirrorPool {
     std::mutex mu;
-    std::unordered_map<const void*, std::pair<void*, size_t>> map;
-    size_t total = 0;
+    std::multimap<size_t, void*> idle;   // capacity -> buffer
+    size_t idle_bytes = 0;
     static constexpr size_t LIMIT = size_t(16) << 30;
 
-    int get(const void* h, size_t bytes, void** d)
+    int acquire(size_t bytes, void** d, size_t* cap)
     {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = map.find(h);
-        if (it != map.end() && it->second.second >= bytes) {
-            *d = it->second.first;
-            return SE_OK;
-        }
-        if (it != map.end()) {
-            cudaFree(it->second.first);
-            total -= it->second.second;
-            map.erase(it);
-        }
-        if (total + bytes > LIMIT) {   // drop every other mirror
-            for (auto& kv : map) cudaFree(kv.second.first);
-            map.clear();
-            total = 0;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            auto it = idle.lower_bound(bytes);
+            if (it != idle.end() && it->first <= 2 * bytes) {   // best fit, at most 2x
+                *d = it->second;
+                *cap = it->first;
+                idle_bytes -= it->first;
+                idle.erase(it);
+                return SE_OK;
+            }
         }
         void* p = nullptr;
         cudaError_t e = cudaMalloc(&p, bytes);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(mirror)", __FILE__, __LINE__);
-        map[h] = {p, bytes};
-        total += bytes;
         *d = p;
+        *cap = bytes;
         return SE_OK;
+    }
+
+    void release(void* d, size_t cap)
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        idle.emplace(cap, d);
+        idle_bytes += cap;
+        while (idle_bytes > LIMIT && !idle.empty()) {
+            auto it = std::prev(idle.end());
+            cudaFree(it->second);
+            idle_bytes -= it->first;
+            idle.erase(it);
+        }
     }
 };
 
-static MirrorCache& mirrors()
+static MirrorPool& mirrors()
 {
-    static MirrorCache* c = new MirrorCache();
+    static MirrorPool* c = new MirrorPool();
     return *c;
 }
 
 // Collects the buffers of one call, copies host inputs in, copies host
-// outputs back at the end.  The same pointer used twice shares one mirror.
+// outputs back at the end (se_hoststage.cu), and returns the device mirrors
+// to the pool when it goes out of scope.  The same pointer used twice shares
+// one mirror.
 class Stager {
 public:
+    Stager() = default;
+    Stager(const Stager&) = delete;
+    Stager& operator=(const Stager&) = delete;
+    ~Stager()
+    {
+        for (auto& e : ents_)
+            if (e.host && e.d) mirrors().release(e.d, e.cap);
+    }
     void* use(const void* h, size_t bytes, bool in, bool out)
     {
         if (!h || bytes == 0 || err_) return nullptr;
@@ -120,15 +146,19 @@ public:
             if (e.h == h) {
                 if (bytes > e.bytes) {   // grow: take a larger mirror
                     e.bytes = bytes;
-                    if (e.host && (err_ = mirrors().get(h, bytes, &e.d))) return nullptr;
+                    if (e.host && bytes > e.cap) {
+                        mirrors().release(e.d, e.cap);
+                        e.d = nullptr;
+                        if ((err_ = mirrors().acquire(bytes, &e.d, &e.cap))) return nullptr;
+                    }
                 }
                 e.in |= in;
                 e.out |= out;
                 return e.d;
             }
-        Ent e{h, nullptr, bytes, !on_device(h), in, out};
+        Ent e{h, nullptr, bytes, 0, !on_device(h), in, out};
         if (e.host) {
-            if ((err_ = mirrors().get(h, bytes, &e.d))) return nullptr;
+            if ((err_ = mirrors().acquire(bytes, &e.d, &e.cap))) return nullptr;
         } else {
             e.d = const_cast<void*>(h);
         }
@@ -143,7 +173,7 @@ private:
     struct Ent {
         const void* h;
         void* d;
-        size_t bytes;
+        size_t bytes, cap;   // cap: the mirror's size (host arrays)
         bool host, in, out;
     };
     std::vector<Ent> ents_;
@@ -228,7 +258,7 @@ int Stager::copy_in()
     const int zero = 0;
     SE_CUDA(cudaMemcpyToSymbol(g_legacy_err, &zero, sizeof(int)));
     for (auto& e : ents_)
-        if (e.host && e.in) SE_CUDA(cudaMemcpy(e.d, e.h, e.bytes, cudaMemcpyHostToDevice));
+        if (e.host && e.in) SE_TRY(host_to_device(e.d, e.h, e.bytes));
     return SE_OK;
 }
 
@@ -238,8 +268,7 @@ int Stager::finish()
     SE_CUDA(cudaGetLastError());
     SE_CUDA(cudaDeviceSynchronize());
     for (auto& e : ents_)
-        if (e.host && e.out)
-            SE_CUDA(cudaMemcpy(const_cast<void*>(e.h), e.d, e.bytes, cudaMemcpyDeviceToHost));
+        if (e.host && e.out) SE_TRY(device_to_host(const_cast<void*>(e.h), e.d, e.bytes));
     int flag = 0;
     SE_CUDA(cudaMemcpyFromSymbol(&flag, g_legacy_err, sizeof(int)));
     return flag ? SE_ERR_INPUT : SE_OK;

@@ -279,9 +279,13 @@ def test_kspace_legacy(F, M):
     np.testing.assert_array_equal(back, r)
 
 
-@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 10, 9), (32, 32, 32)])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 10, 9), (32, 32, 32), (64, 64, 65),
+                                   (100, 100, 101)])
 def test_fftw_shim(F, shape):
-    """fftw_plan_dft_3d / r2c / c2r on cuFFT against numpy's FFT."""
+    """fftw_plan_dft_3d / r2c / c2r on cuFFT against numpy's FFT.  Arrays of
+    1 MiB and more are staged through the pinned chunks of se_hoststage.cu
+    (the last two shapes: one partial chunk, and two chunks and a partial
+    one), and plans of a shape come back from the plan cache."""
     L = F.lib()
     n0, n1, n2 = shape
     rng = np.random.Generator(np.random.Philox(4))
