@@ -35,7 +35,7 @@
 namespace se {
 namespace {
 
-constexpr size_t STAGE_CHUNK = size_t(8) << 20;   // bytes per pinned buffer
+constexpr size_t STAGE_CHUNK = size_t(4) << 20;   // bytes per pinned buffer
 constexpr size_t STAGE_MIN = size_t(1) << 20;     // smaller copies: cudaMemcpy
 constexpr size_t SLICE_MIN = size_t(256) << 10;   // per host thread and chunk
 

@@ -883,11 +883,67 @@ static int do_int_force_vanilla(double* force, const SE_FGG_work* w, const SE_st
     return s.finish();
 }
 
+// Managed arrays of the workspace and system allocators.  A caller that
+// allocates and frees its workspace on every solve (spectral_ewald() does)
+// would otherwise pay for a fresh managed allocation and its first touch on
+// the device each time: freed arrays go to an idle pool (at most LIMIT bytes,
+// largest freed first beyond that) and later allocations of a similar size
+// take them back, zeroed again.
+struct ManagedPool {
+    std::mutex mu;
+    std::unordered_map<void*, size_t> mine;   // every array this pool handed out
+    std::multimap<size_t, void*> idle;
+    size_t idle_bytes = 0;
+    static constexpr size_t LIMIT = size_t(4) << 30;
+
+    int take(void** p, size_t bytes)
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            auto it = idle.lower_bound(bytes);
+            if (it != idle.end() && it->first <= 2 * bytes) {
+                *p = it->second;
+                idle_bytes -= it->first;
+                idle.erase(it);
+                return SE_OK;
+            }
+        }
+        SE_CUDA(cudaMallocManaged(p, bytes));
+        std::lock_guard<std::mutex> lock(mu);
+        mine[*p] = bytes;
+        return SE_OK;
+    }
+
+    // false: not one of this pool's arrays
+    bool give_back(void* p)
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = mine.find(p);
+        if (it == mine.end()) return false;
+        idle.emplace(it->second, p);
+        idle_bytes += it->second;
+        while (idle_bytes > LIMIT && !idle.empty()) {
+            auto big = std::prev(idle.end());
+            cudaFree(big->second);
+            idle_bytes -= big->first;
+            mine.erase(big->second);
+            idle.erase(big);
+        }
+        return true;
+    }
+};
+
+static ManagedPool& managed_pool()
+{
+    static ManagedPool* m = new ManagedPool();
+    return *m;
+}
+
 static int managed_zeros(void** p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 8;
-    SE_CUDA(cudaMallocManaged(p, bytes));
+    SE_TRY(managed_pool().take(p, bytes));
     SE_CUDA(cudaMemset(*p, 0, bytes));
     SE_CUDA(cudaDeviceSynchronize());
     return SE_OK;
@@ -896,6 +952,7 @@ static int managed_zeros(void** p, size_t bytes)
 static void release(void* p)
 {
     if (!p) return;
+    if (managed_pool().give_back(p)) return;
     if (on_device(p)) cudaFree(p);
     else free(p);
 }
