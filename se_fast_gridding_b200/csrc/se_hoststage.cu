@@ -140,22 +140,22 @@ DeviceStage* stage_for_current_device()
     return s.ok ? &s : nullptr;
 }
 
-bool is_pinned(const void* p)
+}  // namespace
+
+bool host_pinned(const void* p)
 {
     cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     return a.type == cudaMemoryTypeHost;
 }
 
-}  // namespace
-
 int host_to_device(void* d, const void* h, size_t n)
 {
     if (n == 0) return SE_OK;
-    if (n < STAGE_MIN || is_pinned(h)) {
+    if (n < STAGE_MIN || host_pinned(h)) {
         SE_CUDA(cudaMemcpy(d, h, n, cudaMemcpyHostToDevice));
         return SE_OK;
     }
@@ -183,7 +183,7 @@ int host_to_device(void* d, const void* h, size_t n)
 int device_to_host(void* h, const void* d, size_t n)
 {
     if (n == 0) return SE_OK;
-    if (n < STAGE_MIN || is_pinned(h)) {
+    if (n < STAGE_MIN || host_pinned(h)) {
         SE_CUDA(cudaMemcpy(h, d, n, cudaMemcpyDeviceToHost));
         return SE_OK;
     }

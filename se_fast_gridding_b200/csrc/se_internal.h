@@ -45,6 +45,8 @@ int stable_sort(const int* keys, const int* vals_in, int N, int nkeys, int* perm
 // wrote d finished.
 int host_to_device(void* d, const void* h, size_t bytes);
 int device_to_host(void* h, const void* d, size_t bytes);
+// p is page-locked host memory (cudaHostAlloc / cudaHostRegister)
+bool host_pinned(const void* p);
 
 // Device flag a plan's kernels set when a position was not finite (reset at
 // the start of each solve on the plan's stream).

@@ -1864,17 +1864,30 @@ extern "C" int se_solve_host(se_plan p, int N, const double* xh, const double* q
     // The call runs on the plan's own stream, after the work queued on the
     // caller's stream so far, and returns when it is done: the solve between
     // the copies replays the plan's host-entry graph (same device buffers and
-    // stream every call; captured anew when N changes).
+    // stream every call; captured anew when N changes).  Pinned arrays are
+    // copied by the stream itself; pageable ones through the pinned chunks
+    // of host_to_device / device_to_host (threaded host copies), which
+    // finish before the solve is queued and after it has finished.
     cudaStream_t st = p->hs;
+    const bool pin_in = host_pinned(xh) && host_pinned(qh), pin_out = host_pinned(outh);
     SE_CUDA(cudaEventRecord(p->hev, user));
     SE_CUDA(cudaStreamWaitEvent(st, p->hev, 0));
-    SE_CUDA(cudaMemcpyAsync(p->d_x, xh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
-    SE_CUDA(cudaMemcpyAsync(p->d_q, qh, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    if (pin_in) {
+        SE_CUDA(cudaMemcpyAsync(p->d_x, xh, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+        SE_CUDA(cudaMemcpyAsync(p->d_q, qh, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+    } else {
+        SE_CUDA(cudaStreamSynchronize(st));   // the caller's work first, as on the stream
+        SE_TRY(host_to_device(p->d_x, xh, sizeof(double) * 3 * N));
+        SE_TRY(host_to_device(p->d_q, qh, sizeof(double) * N));
+    }
     SE_TRY(plan_set_N(p, N, st));
     SE_TRY(batch_solve(p->b, p->d_x, p->d_q, p->d_out, nullptr, st, 1));
-    SE_CUDA(cudaMemcpyAsync(outh, p->d_out, sizeof(double) * outw * N, cudaMemcpyDeviceToHost, st));
+    if (pin_out)
+        SE_CUDA(cudaMemcpyAsync(outh, p->d_out, sizeof(double) * outw * N,
+                                cudaMemcpyDeviceToHost, st));
     SE_CUDA(cudaMemcpyAsync(p->h_err, p->b->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     SE_CUDA(cudaStreamSynchronize(st));
+    if (!pin_out) SE_TRY(device_to_host(outh, p->d_out, sizeof(double) * outw * N));
     return *p->h_err ? SE_ERR_INPUT : SE_OK;
 }
 

@@ -57,6 +57,33 @@ def test_fp64_matches_reference_spectral_ewald(S, N, P, mode):
     se.close()
 
 
+@pytest.mark.parametrize("N,mode", [(60_000, "force"), (150_000, "potential")])
+def test_solve_host_staged_pageable_and_pinned(S, N, mode):
+    """se_solve_host with host arrays of 1 MiB and more: pageable arrays go
+    through the pinned chunks of the host staging (threaded host copies),
+    pinned ones through the stream; both give the device solve's numbers bit
+    for bit, also with pinned inputs and a pageable output and the reverse."""
+    import oracle as O
+    import torch
+    x, q = O.synthetic_system(N, 1.0, seed=N, charges="uniform")
+    se = S.SpectralEwald(64, 12, 1.0, 10.0, None, mode, "fp32", N)
+    ref = host(se.solve(cuda(x), cuda(q)))
+    np.testing.assert_array_equal(se.solve_host(x, q), ref)        # pageable in and out
+    xp = torch.tensor(x).pin_memory()
+    qp = torch.tensor(q).pin_memory()
+    op = torch.empty(ref.size, dtype=torch.float64).pin_memory()
+    se.solve_host_ptr(N, xp.data_ptr(), qp.data_ptr(), op.data_ptr())   # pinned in and out
+    np.testing.assert_array_equal(op.numpy(), ref)
+    out = np.full(ref.size, np.nan)
+    se.solve_host_ptr(N, xp.data_ptr(), qp.data_ptr(), out.ctypes.data)  # pinned in, pageable out
+    np.testing.assert_array_equal(out, ref)
+    op.fill_(float("nan"))
+    xc, qc = np.ascontiguousarray(x), np.ascontiguousarray(q)
+    se.solve_host_ptr(N, xc.ctypes.data, qc.ctypes.data, op.data_ptr())  # pageable in, pinned out
+    np.testing.assert_array_equal(op.numpy(), ref)
+    se.close()
+
+
 def test_fp64_reference_error_figures(S):
     """abs-RMS vs the direct sum, as test_accuracy prints it."""
     import oracle as O
