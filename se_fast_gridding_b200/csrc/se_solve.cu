@@ -431,6 +431,10 @@ struct se_batch_s {
         int Ep = 0, PL = 0;     // window pitches
         int zb = 1;             // z-adjacent bins per window (1 or 2)
         size_t smem = 0;
+        int nk = 0;             // systems served
+        int units = 0;          // CTAs: the systems' bins / zb
+        int* tab = nullptr;     // device: the nk system indices, then the
+                                // exclusive prefix of their units (nk + 1)
     };
     std::vector<I2Class> i2_cls;
     bool i2_force = false;    // some k_interp2 system is in FORCE mode
@@ -625,6 +629,8 @@ static int batch_free(se_batch b)
     }
     for (auto& e : b->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& c : b->i2_cls)
+        if (c.tab) cudaFree(c.tab);
     void* ptrs[] = {b->sys, b->d_part_prefix, b->d_tile_prefix, b->d_bin_prefix, b->key,
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
                     b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows,
@@ -804,6 +810,27 @@ static int interp2_window(const se_batch_s* b, se_batch_s::I2Class& c, long long
     return SE_OK;
 }
 
+// The units table of launch c (se_batch_s::I2Class::tab) for the systems
+// `members`, uploaded to the device.
+static int interp2_table(se_batch_s* b, se_batch_s::I2Class& c, const std::vector<int>& members)
+{
+    std::vector<int> t(members);
+    int units = 0;
+    for (int i : members) {
+        t.push_back(units);
+        const SysDev& S = b->host_sys[i];
+        const int bins = S.nf[0] * S.nf[1] * S.nf[2];
+        if (bins % c.zb) return SE_ERR_INVALID;   // zb = 2 needs pairs of z bins
+        units += bins / c.zb;
+    }
+    t.push_back(units);
+    c.nk = (int)members.size();
+    c.units = units;
+    SE_CUDA(cudaMalloc(&c.tab, sizeof(int) * t.size()));
+    SE_CUDA(cudaMemcpy(c.tab, t.data(), sizeof(int) * t.size(), cudaMemcpyHostToDevice));
+    return SE_OK;
+}
+
 // The k_interp2 launches of a batch (se_batch_s::i2_cls).
 static int interp2_classes(se_batch_s* b, const se_system* systems, int nsys)
 {
@@ -824,20 +851,28 @@ static int interp2_classes(se_batch_s* b, const se_system* systems, int nsys)
         if (S.path & PATH_BIN_WINDOWS) bin_windows = true;
     }
     b->i2_cls.clear();
+    auto members = [&](int P) {   // the pair-interpolation systems of stencil P (0: all)
+        std::vector<int> v;
+        for (int i = 0; i < nsys; i++)
+            if ((b->host_sys[i].path & PATH_PAIR_INTERP) && (P == 0 || systems[i].P == P))
+                v.push_back(i);
+        return v;
+    };
     if (b->runtime_p) {
-        se_batch_s::I2Class c;
+        b->i2_cls.emplace_back();
+        se_batch_s::I2Class& c = b->i2_cls.back();
         c.P = 0;
         c.Pw = maxP;
         SE_TRY(interp2_window(b, c, np, nb, bin_windows));
-        b->i2_cls.push_back(c);
-        return SE_OK;
+        return interp2_table(b, c, members(0));
     }
     for (const auto& kv : byP) {
-        se_batch_s::I2Class c;
+        b->i2_cls.emplace_back();
+        se_batch_s::I2Class& c = b->i2_cls.back();
         c.P = c.Pw = kv.first;
         c.special = interp2_special(kv.first);
         SE_TRY(interp2_window(b, c, kv.second.first, kv.second.second, bin_windows));
-        b->i2_cls.push_back(c);
+        SE_TRY(interp2_table(b, c, members(kv.first)));
     }
     return SE_OK;
 }
@@ -1310,15 +1345,17 @@ template <typename T, bool FORCE>
 static int launch_interp2_mode(se_batch b, const T* grid, double* out, double* phi,
                                cudaStream_t st)
 {
-    // one launch per class; the CTAs of the other classes' bins return at once
-    const dim3 grd(std::max(b->nbins, 1)), blk(I2_WARPS * 32);
+    // one launch per class, one CTA per unit of its systems' bins
+    const dim3 blk(I2_WARPS * 32);
     const T* rows = static_cast<const T*>(b->rows);
     for (const auto& c : b->i2_cls) {
+        if (c.units == 0) continue;
+        const dim3 grd(c.units);
         const void* fn = interp2_kernel<T, FORCE>(c.Pw, c.special);
         SE_CUDA(raise_smem_limit(fn, c.smem));
         const int P = c.special ? c.Pw : 0;
-#define SE_I2ARGS b->sys, b->d_bin_prefix, b->nsys, b->srec, b->sg, b->perm, rows, b->boff, grid, \
-                  out, phi, c.Ep, c.PL, c.zb, c.P
+#define SE_I2ARGS b->sys, c.tab, c.nk, b->srec, b->sg, b->perm, rows, b->boff, grid, \
+                  out, phi, c.Ep, c.PL, c.zb
         if (P == 8) k_interp2<T, 8, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
         else if (P == 12) k_interp2<T, 12, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
         else if (P == 16) k_interp2<T, 16, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
