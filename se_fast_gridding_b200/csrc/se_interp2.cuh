@@ -303,15 +303,15 @@ __device__ __forceinline__ void interp2_columns(
 // with a FORCE system runs this variant; each stores what its mode asks).
 // A launch serves the systems of one stencil (a batch of several stencils
 // runs one launch per stencil, each with its window), one CTA per unit of zb
-// z-adjacent bins: tab holds the nk systems' indices, then the exclusive
-// prefix of their units (nk + 1 entries).  zb = 2: a bin with an even z
+// z-adjacent bins: tab[u] is unit u's system and tab[units + u] its first
+// bin (units = the grid size).  zb = 2: a bin with an even z
 // index and the next one (its z neighbour: nf[2] is even for these systems)
 // share one window of 7 + P x 7 + P x 16 + P cells.  Each particle sums the
 // same window cells in the same pairs either way (its offset in the window
 // moves by 8 cells in z), so the results do not depend on zb.
 template <typename T, int PT, bool FORCE>
 __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_interp2(
-    const SysDev* __restrict__ sys, const int* __restrict__ tab, int nk,
+    const SysDev* __restrict__ sys, const int* __restrict__ tab,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const int* __restrict__ sperm, const T* __restrict__ rows, const int* __restrict__ boff,
     const T* __restrict__ grid, double* __restrict__ out, double* __restrict__ phi_out,
@@ -321,19 +321,12 @@ __global__ void __launch_bounds__(I2_WARPS * 32, sizeof(T) == 4 ? 3 : 2) k_inter
     using VT = typename PV::V;
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ Interp2Warp<T> wsm[I2_WARPS];
-    // the unit's system: the largest k with prefix[k] <= unit
+    // the unit's system and first bin: two independent loads
     const int unit = blockIdx.x;
-    const int* pre = tab + nk;
-    int k = 0;
-    for (int hi = nk - 1; k < hi;) {
-        const int mid = (k + hi + 1) >> 1;
-        if (__ldg(pre + mid) <= unit) k = mid;
-        else hi = mid - 1;
-    }
-    const SysDev& S = sys[__ldg(tab + k)];
-    const int lb = (unit - __ldg(pre + k)) * zb;   // the unit's first bin in the system
-    const int bin = S.bin_base + lb;
+    const int bin = __ldg(tab + gridDim.x + unit);
     const int beg = boff[bin], end = boff[bin + zb];
+    const SysDev& S = sys[__ldg(tab + unit)];
+    const int lb = bin - S.bin_base;   // the unit's first bin in the system
     if (beg == end) return;
     const int P = PT ? PT : S.P;
     const int M = S.M;

@@ -407,6 +407,8 @@ struct se_batch_s {
     // per-tile completion counters, the block counter of k_tile_parts, the
     // FP64 slabs of the parts after the first, and the launch bound
     int* tile_parts = nullptr;
+    int* part_tile = nullptr;   // the tile of each part (written by k_tile_parts)
+    int* tile_sys = nullptr;    // the system of each tile
     int* tile_done = nullptr;
     unsigned* tp_counter = nullptr;
     double* slab = nullptr;
@@ -431,10 +433,8 @@ struct se_batch_s {
         int Ep = 0, PL = 0;     // window pitches
         int zb = 1;             // z-adjacent bins per window (1 or 2)
         size_t smem = 0;
-        int nk = 0;             // systems served
         int units = 0;          // CTAs: the systems' bins / zb
-        int* tab = nullptr;     // device: the nk system indices, then the
-                                // exclusive prefix of their units (nk + 1)
+        int* tab = nullptr;     // device: each unit's system, then its first bin
     };
     std::vector<I2Class> i2_cls;
     bool i2_force = false;    // some k_interp2 system is in FORCE mode
@@ -635,7 +635,7 @@ static int batch_free(se_batch b)
                     b->rec, b->gpk, b->perm, b->srec, b->sg, b->boff, b->sort_scratch,
                     b->grid, b->spec, b->energy_partial, b->err, b->fac, b->rows,
                     b->grid32, b->spec32, b->d_order, b->fft_tw, b->tile_parts,
-                    b->tile_done, b->tp_counter, b->slab};
+                    b->tile_done, b->tp_counter, b->slab, b->part_tile, b->tile_sys};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete b;
@@ -811,21 +811,24 @@ static int interp2_window(const se_batch_s* b, se_batch_s::I2Class& c, long long
 }
 
 // The units table of launch c (se_batch_s::I2Class::tab) for the systems
-// `members`, uploaded to the device.
+// `members`: every unit's system index, then every unit's first (global)
+// bin, uploaded to the device.
 static int interp2_table(se_batch_s* b, se_batch_s::I2Class& c, const std::vector<int>& members)
 {
-    std::vector<int> t(members);
-    int units = 0;
+    std::vector<int> usys, ubin;
     for (int i : members) {
-        t.push_back(units);
         const SysDev& S = b->host_sys[i];
         const int bins = S.nf[0] * S.nf[1] * S.nf[2];
         if (bins % c.zb) return SE_ERR_INVALID;   // zb = 2 needs pairs of z bins
-        units += bins / c.zb;
+        for (int lb = 0; lb < bins; lb += c.zb) {
+            usys.push_back(i);
+            ubin.push_back(S.bin_base + lb);
+        }
     }
-    t.push_back(units);
-    c.nk = (int)members.size();
-    c.units = units;
+    c.units = (int)usys.size();
+    std::vector<int> t(usys);
+    t.insert(t.end(), ubin.begin(), ubin.end());
+    if (t.empty()) return SE_OK;
     SE_CUDA(cudaMalloc(&c.tab, sizeof(int) * t.size()));
     SE_CUDA(cudaMemcpy(c.tab, t.data(), sizeof(int) * t.size(), cudaMemcpyHostToDevice));
     return SE_OK;
@@ -1008,6 +1011,12 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
             if (b->host_sys[i].path & PATH_TILE_SPREAD) ntile2 += systems[i].N;
         b->slab_slots = split_slots(ntile2);
         SE_ALLOC(b->tile_parts, sizeof(int) * (b->ntiles + 1));
+        SE_ALLOC(b->part_tile, sizeof(int) * (size_t)(b->ntiles + b->slab_slots));
+        SE_ALLOC(b->tile_sys, sizeof(int) * std::max(b->ntiles, 1));
+        {   // every entry a valid tile from the start (k_tile_parts rewrites them per solve)
+            const cudaError_t z = cudaMemset(b->part_tile, 0, sizeof(int) * (size_t)(b->ntiles + b->slab_slots));
+            if (z != cudaSuccess) return fail(cuda_fail(z, "cudaMemset", __FILE__, __LINE__));
+        }
         SE_ALLOC(b->tile_done, sizeof(int) * std::max(b->ntiles, 1));
         SE_ALLOC(b->tp_counter, sizeof(unsigned));
         SE_ALLOC(b->slab, sizeof(double) * 4096 * (size_t)b->slab_slots);
@@ -1043,6 +1052,12 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_bin_prefix, b->bin_prefix.data(), sizeof(int) * (nsys + 1),
                        cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && b->tile_sys) {
+        std::vector<int> ts(std::max(b->ntiles, 1), 0);
+        for (int i = 0; i < nsys; i++)
+            for (int t = b->tile_prefix[i]; t < b->tile_prefix[i + 1]; t++) ts[t] = i;
+        e = cudaMemcpy(b->tile_sys, ts.data(), sizeof(int) * ts.size(), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemset(b->err, 0, sizeof(int));
     if (e == cudaSuccess && b->tile_done)
         e = cudaMemset(b->tile_done, 0, sizeof(int) * std::max(b->ntiles, 1));
@@ -1162,24 +1177,26 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
 {
     // every tile is written by exactly one of the two kernels (by system)
     if (b->any_spread2) {
-        // the parts of each tile, then one CTA per part (at most the bound;
-        // the CTAs past the number of parts return at once)
+        // the parts of each tile and each part's tile, then one CTA per part
+        // (at most the bound; the CTAs past the number of parts return at once)
         const int bound = b->ntiles + b->slab_slots;
         k_tile_parts<<<ceil_div(b->ntiles, TP_TILES), TP_WARPS * 32, 0, st>>>(
             b->sys, b->d_tile_prefix, b->nsys, b->ntiles, b->boff, b->tile_parts, b->tp_counter,
-            bound, b->err);
+            bound, b->err, b->part_tile);
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
         if (b->precision == SE_FP32)
             (b->spread2_few ? k_spread2<float, S2_BLOCKS_FEW> : k_spread2<float, S2_BLOCKS_MANY>)
                 <<<bound * S2_CTA_SPLIT, S2_THREADS, 0, st>>>(
-                    b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
-                    static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
+                    b->sys, b->tile_sys, b->srec, b->sg,
+                    static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts,
+                    b->part_tile, b->ntiles,
                     b->tile_done, b->slab, b->slab_slots, b->err);
         else
             k_spread2<double, S2_BLOCKS_FP64><<<bound * S2_CTA_SPLIT, S2_THREADS, 0, st>>>(
-                b->sys, b->d_tile_prefix, b->nsys, b->srec, b->sg,
-                static_cast<const double*>(b->rows), b->boff, grid, b->tile_parts, b->ntiles,
+                b->sys, b->tile_sys, b->srec, b->sg,
+                static_cast<const double*>(b->rows), b->boff, grid, b->tile_parts,
+                b->part_tile, b->ntiles,
                 b->tile_done, b->slab, b->slab_slots, b->err);
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
@@ -1354,7 +1371,7 @@ static int launch_interp2_mode(se_batch b, const T* grid, double* out, double* p
         const void* fn = interp2_kernel<T, FORCE>(c.Pw, c.special);
         SE_CUDA(raise_smem_limit(fn, c.smem));
         const int P = c.special ? c.Pw : 0;
-#define SE_I2ARGS b->sys, c.tab, c.nk, b->srec, b->sg, b->perm, rows, b->boff, grid, \
+#define SE_I2ARGS b->sys, c.tab, b->srec, b->sg, b->perm, rows, b->boff, grid, \
                   out, phi, c.Ep, c.PL, c.zb
         if (P == 8) k_interp2<T, 8, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);
         else if (P == 12) k_interp2<T, 12, FORCE><<<grd, blk, c.smem, st>>>(SE_I2ARGS);

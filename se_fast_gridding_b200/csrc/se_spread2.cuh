@@ -285,7 +285,7 @@ __device__ __forceinline__ int block_candidates(const SysDev& S, int lt, int w,
 // max(1, ceil(candidates of the most crowded block / S2_CAP)) for the
 // k_spread2 systems, 1 for the others), then, in the block that finishes
 // last, their exclusive scan in place: parts[t] = the first part of tile t,
-// parts[ntiles] = the number of parts.  More parts than the launch bound
+// parts[ntiles] = the number of parts, and part_tile[s] = the tile of part s.  More parts than the launch bound
 // (which no input reaches: a bin is a candidate of at most two tiles per
 // axis) set bit 2 of err.  The block counter is left at zero for the next
 // launch.
@@ -294,7 +294,8 @@ constexpr int TP_TILES = TP_WARPS / S2_WARPS;   // tiles per CTA
 
 __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys, int ntiles,
-    const int* __restrict__ boff, int* parts, unsigned* counter, int bound, int* err)
+    const int* __restrict__ boff, int* parts, unsigned* counter, int bound, int* err,
+    int* __restrict__ part_tile)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tile = blockIdx.x * TP_TILES + warp / S2_WARPS, wb = warp % S2_WARPS;
@@ -357,15 +358,22 @@ __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
         if (carry > bound) atomicOr(err, 2);
         *counter = 0u;
     }
+    // every part's tile, for k_spread2 (the first `bound` parts)
+    __syncthreads();
+    for (int t = threadIdx.x; t < ntiles; t += blockDim.x) {
+        const int a = __ldcg(parts + t), b = min(__ldcg(parts + t + 1), bound);
+        for (int s = a; s < b; s++) part_tile[s] = t;
+    }
 }
 
 template <typename Acc, int BLOCKS>
 __global__ void __launch_bounds__(S2_THREADS, BLOCKS * S2_CTA_SPLIT) k_spread2(
-    const SysDev* __restrict__ sys, const int* __restrict__ tile_prefix, int nsys,
+    const SysDev* __restrict__ sys, const int* __restrict__ tile_sys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid,
-    const int* __restrict__ tile_parts, int ntiles, int* __restrict__ tile_done,
-    double* __restrict__ slab, int slab_slots, int* __restrict__ err)
+    const int* __restrict__ tile_parts, const int* __restrict__ part_tile, int ntiles,
+    int* __restrict__ tile_done, double* __restrict__ slab, int slab_slots,
+    int* __restrict__ err)
 {
     constexpr bool FOLD = sizeof(Acc) == 4;
     constexpr int G = s2_group<Acc>();
@@ -373,22 +381,20 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS * S2_CTA_SPLIT) k_spread2(
     __shared__ __align__(16) Spread2Smem<Acc> sm;
     __shared__ int folds;   // this CTA finished its tile's parts last
 
-    // ---- the part this CTA sums: tile = the last t with tile_parts[t] <= item
-    // (warp blocks sub S2_CTA_WARPS + [0, S2_CTA_WARPS) of it)
+    // ---- the part this CTA sums and its tile (k_tile_parts' part_tile; warp
+    // blocks sub S2_CTA_WARPS + [0, S2_CTA_WARPS) of it), and the tile's system
     const int item = blockIdx.x / S2_CTA_SPLIT, sub = blockIdx.x % S2_CTA_SPLIT;
-    if (item >= tile_parts[ntiles]) return;
-    int tile = 0;
-    {
-        int hi = ntiles - 1;
-        while (tile < hi) {
-            const int mid = (tile + hi + 1) >> 1;
-            if (tile_parts[mid] <= item) tile = mid;
-            else hi = mid - 1;
-        }
+    const int nall = tile_parts[ntiles];
+    const int tile = part_tile[item];   // (the grid holds at most `bound` parts)
+    if (item >= nall) return;
+    if ((unsigned)tile >= (unsigned)ntiles) {   // cannot happen: flagged, nothing summed
+        if (threadIdx.x == 0) atomicOr(err, 2);
+        return;
     }
-    const int ipart = item - tile_parts[tile];
-    const int nparts = tile_parts[tile + 1] - tile_parts[tile];
-    const SysDev& S = sys[find_sys(tile_prefix, nsys, tile)];
+    const int first = tile_parts[tile];
+    const int ipart = item - first;
+    const int nparts = tile_parts[tile + 1] - first;
+    const SysDev& S = sys[tile_sys[tile]];
     if (!(S.path & PATH_TILE_SPREAD)) return;   // k_spread covers this system
     const int slot0 = tile_parts[tile] - tile;   // slab slot of part 1
     if (ipart > 0 && slot0 + ipart - 1 >= slab_slots) {   // cannot happen: see k_tile_parts
