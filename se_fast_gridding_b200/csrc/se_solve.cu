@@ -17,9 +17,10 @@
 //               P <= 16; k_spread (se_spread.cuh) for the others
 //   cuFFT D2Z, k_scale (Z of scaling(), SE_general.c:145-175, applied to the
 //               half spectrum as product_rc does, SE_general.c:336-362), Z2D
-//   interp      k_grid_to_f32 (FP32 path) + k_interp2, one CTA per fine bin,
-//               the unfold fused (se_interp2.cuh), beside k_spread2;
-//               k_interp (se_interp.cuh) for the others
+//   interp      k_grid_to_f32 (FP32 path) + k_interp2, one launch per stencil
+//               of the batch, one CTA per fine bin or pair of z-adjacent bins
+//               of its systems, the unfold fused (se_interp2.cuh), beside
+//               k_spread2; k_interp (se_interp.cuh) for the others
 //
 // Grid layout: M^3 FP64 row-major [x][y][z], the transpose of the reference's
 // column-major H_per; the FFT of the transpose is the transpose of the FFT and
