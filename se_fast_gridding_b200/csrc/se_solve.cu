@@ -1107,6 +1107,9 @@ static int batch_create(se_batch* out, const se_system* systems, int nsys, int p
             a = cudaFuncSetAttribute((const void*)k_spread2<float, S2_BLOCKS_FEW>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         if (a == cudaSuccess)
+            a = cudaFuncSetAttribute((const void*)k_spread2<float, S2_BLOCKS_MANY, 1>,
+                                     cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+        if (a == cudaSuccess)
             a = cudaFuncSetAttribute((const void*)k_spread2<double, S2_BLOCKS_FP64>,
                                      cudaFuncAttributePreferredSharedMemoryCarveout, carve);
         if (a != cudaSuccess) return fail(cuda_fail(a, "cudaFuncSetAttribute", __FILE__, __LINE__));
@@ -1186,15 +1189,21 @@ static int run_spread(se_batch b, double* grid, cudaStream_t st)
             bound, b->err, b->part_tile);
         SE_CUDA(cudaGetLastError());
         LAUNCHED(b);
-        if (b->precision == SE_FP32)
+        constexpr int SPLIT = S2_WARPS / S2_CTA_WARPS;
+        if (b->precision == SE_FP32 && !b->spread2_few && b->ntiles >= S2_ONE_WARP_TILES)
+            k_spread2<float, S2_BLOCKS_MANY, 1><<<bound * S2_WARPS, 32, 0, st>>>(
+                b->sys, b->tile_sys, b->srec, b->sg, static_cast<const float*>(b->rows), b->boff,
+                grid, b->tile_parts, b->part_tile, b->ntiles, b->tile_done, b->slab,
+                b->slab_slots, b->err);
+        else if (b->precision == SE_FP32)
             (b->spread2_few ? k_spread2<float, S2_BLOCKS_FEW> : k_spread2<float, S2_BLOCKS_MANY>)
-                <<<bound * S2_CTA_SPLIT, S2_THREADS, 0, st>>>(
+                <<<bound * SPLIT, S2_CTA_WARPS * 32, 0, st>>>(
                     b->sys, b->tile_sys, b->srec, b->sg,
                     static_cast<const float*>(b->rows), b->boff, grid, b->tile_parts,
                     b->part_tile, b->ntiles,
                     b->tile_done, b->slab, b->slab_slots, b->err);
         else
-            k_spread2<double, S2_BLOCKS_FP64><<<bound * S2_CTA_SPLIT, S2_THREADS, 0, st>>>(
+            k_spread2<double, S2_BLOCKS_FP64><<<bound * SPLIT, S2_CTA_WARPS * 32, 0, st>>>(
                 b->sys, b->tile_sys, b->srec, b->sg,
                 static_cast<const double*>(b->rows), b->boff, grid, b->tile_parts,
                 b->part_tile, b->ntiles,

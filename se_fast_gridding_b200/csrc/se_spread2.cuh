@@ -61,9 +61,14 @@ constexpr int S2_WARPS = 4;   // warp blocks per tile
 #define SE_S2_CTA_WARPS 2
 #endif
 constexpr int S2_CTA_WARPS = SE_S2_CTA_WARPS;
-constexpr int S2_CTA_SPLIT = S2_WARPS / S2_CTA_WARPS;   // CTAs per part of a tile
-constexpr int S2_THREADS = S2_CTA_WARPS * 32;
 static_assert(S2_WARPS % S2_CTA_WARPS == 0, "a tile's warp blocks split evenly into CTAs");
+// grids of at least S2_ONE_WARP_TILES tiles (the 5-CTA build) run one warp
+// per CTA instead (the M = 512 clustered spread 11.48 -> 11.13 ms; smaller
+// grids measured better with two)
+#ifndef SE_S2_ONE_WARP_TILES
+#define SE_S2_ONE_WARP_TILES 32768
+#endif
+constexpr int S2_ONE_WARP_TILES = SE_S2_ONE_WARP_TILES;
 constexpr int S2_LIST = 64;    // per-class list ring: >= group - 1 + 32
 constexpr int S2_SEGS = 64;    // bin segments reaching a warp's block: <= 5 x 4 x 2 for P <= 16
 constexpr int S2_FOLD = 512;   // FP32 partial sums cover this many of a warp's particles
@@ -88,12 +93,12 @@ struct Spread2Stage {
     double q[s2_group<Acc>()];
 };
 
-template <typename Acc>
+template <typename Acc, int CW>
 struct Spread2Smem {
-    Spread2Stage<Acc> stage[S2_CTA_WARPS][2];
-    int2 list[S2_CTA_WARPS][S2_CLASSES][S2_LIST];   // (particle, packed grid index)
-    int seg_beg[S2_CTA_WARPS][S2_SEGS];
-    int seg_pre[S2_CTA_WARPS][S2_SEGS];
+    Spread2Stage<Acc> stage[CW][2];
+    int2 list[CW][S2_CLASSES][S2_LIST];   // (particle, packed grid index)
+    int seg_beg[CW][S2_SEGS];
+    int seg_pre[CW][S2_SEGS];
 };
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc)
@@ -366,8 +371,9 @@ __global__ void __launch_bounds__(TP_WARPS * 32) k_tile_parts(
     }
 }
 
-template <typename Acc, int BLOCKS>
-__global__ void __launch_bounds__(S2_THREADS, BLOCKS * S2_CTA_SPLIT) k_spread2(
+// CW warps per CTA (S2_WARPS / CW CTAs per part of a tile)
+template <typename Acc, int BLOCKS, int CW = S2_CTA_WARPS>
+__global__ void __launch_bounds__(CW * 32, BLOCKS * (S2_WARPS / CW)) k_spread2(
     const SysDev* __restrict__ sys, const int* __restrict__ tile_sys,
     const double4* __restrict__ srec, const int* __restrict__ sg,
     const Acc* __restrict__ rows, const int* __restrict__ boff, double* __restrict__ grid,
@@ -378,11 +384,12 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS * S2_CTA_SPLIT) k_spread2(
     constexpr bool FOLD = sizeof(Acc) == 4;
     constexpr int G = s2_group<Acc>();
     constexpr int V = 16 / sizeof(Acc);   // entries per 16-byte copy
-    __shared__ __align__(16) Spread2Smem<Acc> sm;
+    constexpr int S2_CTA_SPLIT = S2_WARPS / CW, S2_THREADS = CW * 32;
+    __shared__ __align__(16) Spread2Smem<Acc, CW> sm;
     __shared__ int folds;   // this CTA finished its tile's parts last
 
     // ---- the part this CTA sums and its tile (k_tile_parts' part_tile; warp
-    // blocks sub S2_CTA_WARPS + [0, S2_CTA_WARPS) of it), and the tile's system
+    // blocks sub CW + [0, CW) of it), and the tile's system
     const int item = blockIdx.x / S2_CTA_SPLIT, sub = blockIdx.x % S2_CTA_SPLIT;
     const int nall = tile_parts[ntiles];
     const int tile = part_tile[item];   // (the grid holds at most `bound` parts)
@@ -406,7 +413,7 @@ __global__ void __launch_bounds__(S2_THREADS, BLOCKS * S2_CTA_SPLIT) k_spread2(
     const int tix = lt / (nt * nt), tiy = (lt / nt) % nt, tiz = lt % nt;
     const int x0 = tix * 16, y0 = tiy * 16, z0 = tiz * 16;
     const int t = threadIdx.x, lw = t >> 5, lane = t & 31;
-    const int warp = sub * S2_CTA_WARPS + lw;   // the warp block of the tile
+    const int warp = sub * CW + lw;   // the warp block of the tile
     const int wy = warp >> 1, wz = warp & 1;
     const int ly = lane >> 2, lz = (lane & 3) * 2;
     const unsigned ybits = 0xFFu << (8 * wy), zbits = 0xFFu << (8 * wz);

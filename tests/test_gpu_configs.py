@@ -185,3 +185,22 @@ def test_c5_scaled_against_direct_sum(env, c5):
     assert e64 < 5e-6, e64
     assert abs(e32 - e64) < FP32_TOL, (e32, e64)
     assert rel(out["fp32"], out["fp64"]) < FP32_TOL, rel(out["fp32"], out["fp64"])
+
+
+def test_large_grid_one_warp_spread_ctas(env):
+    """Grids of 32,768 tiles and more (M = 512) run the tile spread with one
+    warp per CTA: clustered FORCE particles at P = 12 (the 16M-particle
+    system's grid, xi and cluster width, 400k particles) in FP32 within 1e-6
+    of FP64, and deterministic."""
+    import oracle as O
+    torch, S, W = env
+    N, M, P, L, xi = 400_000, 512, 12, 1.0, 60.0
+    x, q = W.synthetic_system(N, L, seed=512, charges="pm1", clusters=64, sigma=0.02)
+    xd, qd = torch.tensor(x, device="cuda"), torch.tensor(q, device="cuda")
+    out = {}
+    for prec in ("fp64", "fp32"):
+        se = S.SpectralEwald(M, P, L, xi, None, "force", prec, N)
+        out[prec] = host(se.solve(xd, qd))
+        np.testing.assert_array_equal(host(se.solve(xd, qd)), out[prec])
+        se.close()
+    assert rel(out["fp32"], out["fp64"]) < FP32_TOL, rel(out["fp32"], out["fp64"])
